@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Benchmark of qcu's hot path on B200: even-odd preconditioned BiCGSTAB for
+the Wilson operator on a 32^3 x 64 lattice.
+
+Workload (one "step" = one full solve):
+  * lattice 32x32x32x64, antiperiodic in t, smooth SU(3) links
+    U = exp(i eps H), eps = 0.25, reunitarised (seeded, generated on the GPU
+    by the library's own generator);
+  * source: complex normal N(0,1) per component (seeded);
+  * kappa chosen so the plain FP64 BiCGSTAB needs about 1000 iterations;
+  * stop at a true relative residual ||b - M x|| / ||b|| <= 1e-10, recomputed
+    in FP64 on the full two-parity system at the end of every solve.
+Timed: the chosen solver (mixed precision with FP64 reliable updates).  The
+plain FP64 BiCGSTAB on the same GPU, the dslash bandwidth and a CPU baseline
+(the FP64 CPU oracle, all host cores, bounded sample) are reported beside it.
+
+Multi-GPU: the path does not shard in this implementation (replicas only):
+every rank solves its own seeded system; the time is the max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LATT = [32, 32, 32, 64]
+EPS = 0.25
+T_BC = -1.0
+GAUGE_SEED = 20251203
+SRC_SEED = 7
+KAPPA = 0.1295            # plain FP64 BiCGSTAB: about 1000 iterations on this ensemble
+PLAIN_ITERS_REF = 1000    # iteration count used to extrapolate the CPU sample when no GPU run is available
+TOL = 1e-10
+METRIC = "solve s to 1e-10 true residual, chosen vs plain FP64, 1 B200; dslash HBM GB/s"
+# algorithmic bytes per output site of the hopping term (in-spinor + 8 recon-12 links + out-spinor)
+DSLASH_BYTES = {64: 192 + 8 * 96 + 192, 32: 96 + 8 * 48 + 96, 16: 52 + 8 * 24 + 52}
+DSLASH_FLOPS = 1320
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", type=int, default=16, choices=[16, 32, 64], help="inner precision of the chosen solver")
+    ap.add_argument("--kappa", type=float, default=KAPPA)
+    ap.add_argument("--latt", type=int, nargs=4, default=LATT)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            ident = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        except Exception:
+            ident = str(self.dev)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={ident}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [v.strip() for v in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_sample(latt, kappa, gauge_np, b_np, plain_iters, budget_s=12.0):
+    """FP64 CPU oracle (OpenMP, all host threads) on a bounded number of
+    BiCGSTAB iterations of the same system, extrapolated to plain_iters."""
+    import numpy as np
+
+    import oracle as O
+
+    threads = O.get_threads()
+    bo = np.ascontiguousarray(b_np[1])
+    t0 = time.perf_counter()
+    O.bicgstab(bo, gauge_np, latt, kappa, t_bc=T_BC, tol=1e-30, maxiter=1)
+    t1 = time.perf_counter() - t0
+    n = max(2, min(50, int(budget_s / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    _, it, _ = O.bicgstab(bo, gauge_np, latt, kappa, t_bc=T_BC, tol=1e-30, maxiter=n)
+    dt = time.perf_counter() - t0
+    per_iter = dt / max(it, 1)
+    return {"value": per_iter * plain_iters, "unit": "s", "cores": threads, "kind": "port",
+            "sample": f"{it} FP64 BiCGSTAB iterations of the CPU oracle on {'x'.join(map(str, latt))} "
+                      f"({dt:.1f} s, {per_iter:.3f} s/iteration), extrapolated to {plain_iters} iterations",
+            "seconds_per_iteration": per_iter}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, v, device=None):
+    if pg is None:
+        return v
+    import torch
+
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, world, rank, pg):
+    """Reference arm: the CPU restatement of qcu's algorithm (FP64 BiCGSTAB,
+    OpenMP, all host threads) on a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    import numpy as np
+
+    import oracle as O
+
+    latt = list(args.latt)
+    U = O.gauge_smooth(latt, EPS, GAUGE_SEED)
+    b = O.fermion_gauss(O.full_shape(latt), SRC_SEED)
+    cb = cpu_sample(latt, args.kappa, U, b, PLAIN_ITERS_REF, budget_s=max(5.0, 60.0 / max(args.steps + args.warmup, 1)))
+    line = {"metric": METRIC, "value": cb["value"], "unit": "s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["value"] * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic (seeded)",
+            "config": {"workload": "wilson-bicgstab-32^3x64-smooth-eps0.25", "latt": latt, "kappa": args.kappa,
+                       "tol": TOL, "t_boundary": T_BC},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local, pg):
+    import numpy as np
+    import torch
+
+    import qcu_b200 as q
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    latt = list(args.latt)
+    L = q.Layout(tuple(latt))
+    gauge = torch.empty(L.gauge, dtype=torch.complex128, device=dev)
+    q.gauge_random(gauge, latt, 1, EPS, GAUGE_SEED + rank)
+    b = torch.empty(L.full, dtype=torch.complex128, device=dev)
+    q.fermion_random(b, b.numel(), 0, SRC_SEED + rank)
+    x = torch.empty_like(b)
+    G = q.Gauge(gauge, latt, t_boundary=T_BC)
+    lib_stream = torch.cuda.ExternalStream(q.stream_handle(), device=dev)
+
+    def timed_solve(prec, delta):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(lib_stream)
+        info = G.invert(x, b, args.kappa, tol=TOL, maxiter=20000, precision=prec, delta=delta)
+        e1.record(lib_stream)
+        e1.synchronize()
+        if info["status"] != 1 or info["true_residual"] > TOL:
+            raise RuntimeError(f"solve failed: {info}")
+        return e0.elapsed_time(e1) / 1e3, info
+
+    # plain FP64 BiCGSTAB (reliable update only at the end = true-residual check)
+    plain_t, plain_info = timed_solve(64, 0.0)
+    plain_t = min(plain_t, timed_solve(64, 0.0)[0])
+    # chosen solver: warm-up then K timed solves
+    for _ in range(args.warmup):
+        timed_solve(args.precision, 0.1)
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = q.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(lib_stream)
+    infos = []
+    for _ in range(args.steps):
+        infos.append(G.invert(x, b, args.kappa, tol=TOL, maxiter=20000, precision=args.precision, delta=0.1))
+    e1.record(lib_stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    launches = q.kernel_launches() - launches0
+    clk = clocks.stop()
+    total = e0.elapsed_time(e1) / 1e3
+    for info in infos:
+        if info["status"] != 1 or info["true_residual"] > TOL:
+            raise RuntimeError(f"chosen solve failed: {info}")
+    total = max_over_ranks(pg, total, dev)
+    per_solve = total / args.steps
+
+    # dslash bandwidth (CUDA events on the library stream)
+    pk, pk_kind = peaks()
+    vh = L.vh
+    dsl = {}
+    for prec in (64, 32, 16):
+        ms = G.bench_dslash(prec, False, 50)
+        dsl[prec] = {"ms": ms, "GBps": DSLASH_BYTES[prec] * vh / (ms * 1e-3) / 1e9,
+                     "TFLOPs": DSLASH_FLOPS * vh / (ms * 1e-3) / 1e12}
+    dom = dsl[args.precision]
+    roofline = {"bound": "hbm", "achieved": round(dom["GBps"], 1), "peak": pk, "unit": "GB/s",
+                "frac": round(dom["GBps"] / pk, 4), "traffic": None,
+                "kernel": f"k_dslash<{ {64: 'SOA64', 32: 'SOA32', 16: 'SOA16'}[args.precision] }> "
+                          f"({DSLASH_BYTES[args.precision]} B/site x {vh} sites per launch)",
+                "peak_kind": pk_kind}
+
+    # end to end through the C ABI with host buffers: H2D gauge + b, load, solve, D2H x
+    e2e = None
+    if not args.no_e2e:
+        hg = gauge.cpu().pin_memory()
+        hb = b.cpu().pin_memory()
+        hx = torch.empty(L.full, dtype=torch.complex128).pin_memory()
+        dg = torch.empty_like(gauge)
+        db = torch.empty_like(b)
+        dx = torch.empty_like(b)
+        times = []
+        for i in range(2):
+            torch.cuda.synchronize()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record()
+            dg.copy_(hg, non_blocking=True)
+            db.copy_(hb, non_blocking=True)
+            with q.Gauge(dg, latt, t_boundary=T_BC) as G2:
+                info = G2.invert(dx, db, args.kappa, tol=TOL, maxiter=20000, precision=args.precision, delta=0.1)
+            hx.copy_(dx, non_blocking=True)
+            s1.record()
+            s1.synchronize()
+            if info["status"] != 1:
+                raise RuntimeError(f"e2e solve failed: {info}")
+            if i > 0:
+                times.append(s0.elapsed_time(s1) / 1e3)
+        e2e_t = max_over_ranks(pg, min(times), dev)
+        e2e = {"value": round(e2e_t, 4), "unit": "s", "h2d_bytes_per_step": hg.numel() * 16 + hb.numel() * 16,
+               "d2h_bytes_per_step": hx.numel() * 16}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cb = cpu_sample(latt, args.kappa, gauge.cpu().numpy(), b.cpu().numpy(), plain_info["iterations"])
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        chosen = infos[-1]
+        line = {
+            "metric": METRIC, "value": round(per_solve, 4), "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(per_solve * 1e3, 2), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {64: "f64", 32: "f32 storage / f64 reductions", 16: "f16+norm storage / f32 math / f64 reductions"}[
+                args.precision],
+            "data": "synthetic (seeded smooth SU(3) gauge, Gaussian source)",
+            "config": {"workload": "wilson-bicgstab-32^3x64-smooth-eps0.25", "latt": latt, "kappa": args.kappa,
+                       "tol": TOL, "t_boundary": T_BC, "solver": f"BiCGSTAB inner {args.precision}-bit, FP64 reliable updates (delta 0.1)",
+                       "parallelism": "replicas" if world > 1 else "single", "l2": "working set (GBs) larger than L2"},
+            "chosen": {"iterations": chosen["iterations"], "reliable_updates": chosen["reliable_updates"],
+                       "true_residual": chosen["true_residual"]},
+            "plain_fp64": {"seconds": round(plain_t, 4), "iterations": plain_info["iterations"],
+                           "true_residual": plain_info["true_residual"]},
+            "speedup_vs_plain_fp64": round(plain_t / per_solve, 3),
+            "dslash": {str(k): {"ms": round(v["ms"], 4), "GBps": round(v["GBps"], 1), "frac_of_peak": round(v["GBps"] / pk, 4),
+                                "TFLOPs": round(v["TFLOPs"], 2)} for k, v in dsl.items()},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    G.close()
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank, pg)
+        else:
+            run_ours(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,98 @@
+/*
+ * qcu_ext.h -- additive extension ABI of the B200 implementation.
+ *
+ * qcu's own ABI (qcu.h) fixes kappa = 0.125, an absolute tolerance, FP64,
+ * periodic boundaries and rebuilds everything on every call.  These entry
+ * points expose the same path with its parameters: a gauge field (and clover
+ * term) loaded once and kept on the device, any kappa, a relative FP64
+ * true-residual tolerance, an inner precision of 64/32/16 bits with reliable
+ * updates, the t boundary phase, and solver statistics.
+ *
+ * Same data conventions as qcu.h: device pointers, complex128, PyQuda layout,
+ * lattice {Lx, Ly, Lz, Lt}, parity = output parity.  Every function returns
+ * 0 on success and a non-zero code on error (1 bad argument, 2 CUDA error,
+ * 3 internal), with the message available from qcuGetLastError().
+ */
+#ifndef QCU_B200_QCU_EXT_H
+#define QCU_B200_QCU_EXT_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct qcuGauge_s *qcuGauge;
+
+/* last error of the calling thread: returns its code, copies the message */
+int qcuGetLastError(char *msg, int len);
+int qcuVersion(void);
+
+/* Load a gauge field (PyQuda layout) onto the device as reconstruct-12
+ * storage in FP64, FP32 and FP16.  t_boundary = +1 periodic, -1 antiperiodic
+ * in time (applied in the stencil, so the links stay SU(3)).  clover_coeff
+ * != 0 also builds the clover term A = 1 - coeff/8 sum_{mu<nu} gamma_mu
+ * gamma_nu (Q_munu - Q_munu^dag) and its inverse on both parities; coeff =
+ * kappa*csw is the Sheikholeslami-Wohlert term, coeff = 1 is qcu's clover
+ * (src/clover_dslash.cu:826-835). */
+int qcuGaugeLoad(qcuGauge *h, const void *gauge, const int latt[4], double t_boundary, double clover_coeff);
+int qcuGaugeFree(qcuGauge h);
+
+/* half spinors: out(parity) = [A_parity^{-1}] D_{parity <- 1-parity} in, computed
+ * with the field stored in `precision` bits (64, 32, or 16 = FP16 + per-site
+ * norm; accumulation in FP64 resp. FP32); input and output stay complex128 */
+int qcuDslash(qcuGauge h, void *out, const void *in, int parity, int use_clover, int precision);
+/* odd-parity Schur operator M_pc = 1 - kappa^2 [A_o^-1] D_oe [A_e^-1] D_eo */
+int qcuMatPC(qcuGauge h, void *out, const void *in, double kappa, int use_clover);
+/* full operator on full spinors, M = A - kappa D (A = 1 for Wilson) */
+int qcuMat(qcuGauge h, void *out, const void *in, double kappa, int use_clover);
+
+typedef struct {
+  double kappa;
+  double tol;            /* stop when ||b - M x|| <= tol ||b|| (FP64, full system) */
+  int maxiter;
+  int precision;         /* inner precision: 64, 32 or 16 (FP16 + per-site norm) */
+  double delta;          /* reliable update threshold (0.1 typical; 0 = only at the end) */
+  int abs_tol;           /* 1: qcu's test, iterated ||r_o||^2 < tol */
+  int x0_mode;           /* 0 zero, 1 use x on input, 2 uniform (0,1] from x0_seed */
+  unsigned long long x0_seed;
+  int use_clover;
+  int chunk;             /* iterations per captured CUDA graph (0 = automatic) */
+} qcuInvertParam;
+
+typedef struct {
+  int iterations;
+  int reliable_updates;
+  int status;            /* 1 converged, 2 max iterations, 3 breakdown, 4 NaN/Inf */
+  int restarts;
+  double true_residual;  /* ||b - M x|| / ||b||, recomputed in FP64 at the end */
+  double iter_residual2; /* last iterated ||r_o||^2 */
+  double seconds;
+} qcuInvertResult;
+
+void qcuInvertParamDefault(qcuInvertParam *p);
+/* x, b: full spinors.  Even-odd preconditioned BiCGSTAB on the odd sites. */
+int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuInvertResult *r);
+
+/* seeded generators, PyQuda layout complex128 on the device.
+ * gauge kind: 0 Haar SU(3), 1 exp(i eps H) reunitarised, 2 unit links.
+ * fermion kind: 0 complex normal N(0,1) per component, 1 uniform (0,1]. */
+int qcuGaugeRandom(void *gauge, const int latt[4], int kind, double eps, unsigned long long seed);
+int qcuFermionRandom(void *psi, long long n_complex, int kind, unsigned long long seed);
+
+/* number of kernels this library has launched in this process (graph
+ * replays count every node) */
+long long qcuKernelLaunches(void);
+
+/* the library's CUDA stream on the current device (for event timing) */
+void *qcuGetStream(void);
+
+/* Kernel timing: `iters` back-to-back applications of the internal-layout
+ * hopping term (precision 64/32/16, optionally with the clover inverse) on
+ * random input, alternating parities, timed with CUDA events on the library
+ * stream.  Returns the mean milliseconds per application. */
+int qcuBenchDslash(qcuGauge h, int precision, int use_clover, int iters, double *ms_per_call);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

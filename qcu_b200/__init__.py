@@ -1,0 +1,285 @@
+"""qcu_b200 -- B200-native implementation of qcu's fermion-matrix hot path.
+
+The product is the shared library ``libqcu.so`` next to this file: sm_100a
+CUDA kernels and C++ host code behind qcu's own C ABI (``include/qcu.h``) and
+an additive extension ABI (``include/qcu_ext.h``).  This module is the Python
+host side.  Its legacy half mirrors PyQuda's ``pyquda.pyqcu`` binding
+(python/PyQuda/pyquda/src/pyqcu.pyx:1-34): a ``QcuParam`` with a
+``lattice_size`` attribute and the six ``*Qcu`` functions taking device
+pointers (anything with a ``.ptr`` attribute, an ``int`` address, or a CUDA
+torch tensor).  The extension half wraps ``qcu_ext.h``.
+
+There is no CPU fallback: importing this module raises if the library is
+missing, and every call goes to the GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libqcu.so")
+
+
+def build(jobs: int = 8) -> str:
+    """Compile libqcu.so for sm_100a (nvcc cross-compiles; no GPU needed)."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", _HERE, f"-j{jobs}"], check=True)
+    return LIB_PATH
+
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {_HERE}` (no CPU fallback exists)")
+
+_lib = ctypes.CDLL(LIB_PATH)
+_vp = ctypes.c_void_p
+
+
+class QcuParam(ctypes.Structure):
+    """``QcuParam`` of include/qcu.h:17-19: ``lattice_size`` is [Lx, Ly, Lz, Lt]."""
+
+    _fields_ = [("_size", ctypes.c_int * 4)]
+
+    def __init__(self, lattice_size=None):
+        super().__init__()
+        if lattice_size is not None:
+            self.lattice_size = lattice_size
+
+    @property
+    def lattice_size(self):
+        return list(self._size)
+
+    @lattice_size.setter
+    def lattice_size(self, value):
+        v = [int(x) for x in value]
+        if len(v) != 4:
+            raise ValueError("lattice_size needs 4 entries")
+        for i in range(4):
+            self._size[i] = v[i]
+
+
+class QcuInvertParam(ctypes.Structure):
+    _fields_ = [
+        ("kappa", ctypes.c_double),
+        ("tol", ctypes.c_double),
+        ("maxiter", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("delta", ctypes.c_double),
+        ("abs_tol", ctypes.c_int),
+        ("x0_mode", ctypes.c_int),
+        ("x0_seed", ctypes.c_ulonglong),
+        ("use_clover", ctypes.c_int),
+        ("chunk", ctypes.c_int),
+    ]
+
+
+class QcuInvertResult(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int),
+        ("reliable_updates", ctypes.c_int),
+        ("status", ctypes.c_int),
+        ("restarts", ctypes.c_int),
+        ("true_residual", ctypes.c_double),
+        ("iter_residual2", ctypes.c_double),
+        ("seconds", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_P = ctypes.POINTER(QcuParam)
+for _name in ("dslashQcu", "dslashCloverQcu"):
+    getattr(_lib, _name).argtypes = [_vp, _vp, _vp, _P, ctypes.c_int]
+    getattr(_lib, _name).restype = None
+_lib.mpiDslashQcu.argtypes = [_vp, _vp, _vp, _P, ctypes.c_int, _P]
+_lib.mpiBistabCgQcu.argtypes = [_vp, _P, _P]
+_lib.ncclDslashQcu.argtypes = [_vp, _vp, _vp, _P, ctypes.c_int, _P]
+_lib.ncclBistabCgQcu.argtypes = [_vp, _vp, _vp, _P, _P]
+for _name in ("mpiDslashQcu", "mpiBistabCgQcu", "ncclDslashQcu", "ncclBistabCgQcu"):
+    getattr(_lib, _name).restype = None
+_lib.qcuGetLastError.argtypes = [ctypes.c_char_p, ctypes.c_int]
+_lib.qcuGetLastError.restype = ctypes.c_int
+_lib.qcuGaugeLoad.argtypes = [ctypes.POINTER(_vp), _vp, ctypes.POINTER(ctypes.c_int), ctypes.c_double, ctypes.c_double]
+_lib.qcuGaugeFree.argtypes = [_vp]
+_lib.qcuDslash.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+_lib.qcuMatPC.argtypes = [_vp, _vp, _vp, ctypes.c_double, ctypes.c_int]
+_lib.qcuMat.argtypes = [_vp, _vp, _vp, ctypes.c_double, ctypes.c_int]
+_lib.qcuInvertParamDefault.argtypes = [ctypes.POINTER(QcuInvertParam)]
+_lib.qcuInvertParamDefault.restype = None
+_lib.qcuInvert.argtypes = [_vp, _vp, _vp, ctypes.POINTER(QcuInvertParam), ctypes.POINTER(QcuInvertResult)]
+_lib.qcuGaugeRandom.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong]
+_lib.qcuFermionRandom.argtypes = [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_ulonglong]
+_lib.qcuGetStream.restype = _vp
+_lib.qcuKernelLaunches.restype = ctypes.c_longlong
+_lib.qcuBenchDslash.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+
+
+class QcuError(RuntimeError):
+    pass
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(1024)
+    code = _lib.qcuGetLastError(buf, 1024)
+    return code, buf.value.decode(errors="replace")
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise QcuError(last_error()[1] or f"qcu error {rc}")
+
+
+def _ptr(x) -> int:
+    """Device address of a Pointer-like (``.ptr``), an int, or a CUDA tensor."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "ptr"):
+        return int(x.ptr)
+    if hasattr(x, "data_ptr"):
+        if not x.is_cuda:
+            raise ValueError("tensor must live on the GPU")
+        if not x.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return int(x.data_ptr())
+    raise TypeError(f"cannot take a device pointer of {type(x)!r}")
+
+
+def _param(p) -> QcuParam:
+    return p if isinstance(p, QcuParam) else QcuParam(p)
+
+
+# ------------------------------------------------------------------ qcu.h (pyqcu mirror)
+def dslashQcu(fermion_out, fermion_in, gauge, param, parity: int) -> None:
+    _lib.dslashQcu(_ptr(fermion_out), _ptr(fermion_in), _ptr(gauge), ctypes.byref(_param(param)), int(parity))
+
+
+def dslashCloverQcu(fermion_out, fermion_in, gauge, param, parity: int) -> None:
+    _lib.dslashCloverQcu(_ptr(fermion_out), _ptr(fermion_in), _ptr(gauge), ctypes.byref(_param(param)), int(parity))
+
+
+def mpiDslashQcu(fermion_out, fermion_in, gauge, param, parity: int, grid) -> None:
+    _lib.mpiDslashQcu(_ptr(fermion_out), _ptr(fermion_in), _ptr(gauge), ctypes.byref(_param(param)), int(parity),
+                      ctypes.byref(_param(grid)))
+
+
+def mpiBistabCgQcu(gauge, param, grid) -> None:
+    _lib.mpiBistabCgQcu(_ptr(gauge), ctypes.byref(_param(param)), ctypes.byref(_param(grid)))
+
+
+def ncclDslashQcu(fermion_out, fermion_in, gauge, param, parity: int, grid) -> None:
+    _lib.ncclDslashQcu(_ptr(fermion_out), _ptr(fermion_in), _ptr(gauge), ctypes.byref(_param(param)), int(parity),
+                       ctypes.byref(_param(grid)))
+
+
+def ncclBistabCgQcu(fermion_out, fermion_in, gauge, param, grid) -> None:
+    _lib.ncclBistabCgQcu(_ptr(fermion_out), _ptr(fermion_in), _ptr(gauge), ctypes.byref(_param(param)),
+                         ctypes.byref(_param(grid)))
+
+
+# ------------------------------------------------------------------ qcu_ext.h
+def _latt(latt):
+    return (ctypes.c_int * 4)(*[int(v) for v in latt])
+
+
+class Gauge:
+    """A gauge field (and optional clover term) resident on the device."""
+
+    def __init__(self, gauge, latt, t_boundary: float = 1.0, clover_coeff: float = 0.0):
+        self.latt = [int(v) for v in latt]
+        self._h = _vp()
+        _check(_lib.qcuGaugeLoad(ctypes.byref(self._h), _ptr(gauge), _latt(self.latt), float(t_boundary),
+                                 float(clover_coeff)))
+        self.t_boundary = t_boundary
+        self.clover_coeff = clover_coeff
+
+    def close(self):
+        if self._h:
+            _lib.qcuGaugeFree(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def dslash(self, out, inp, parity: int, clover: bool = False, precision: int = 64):
+        _check(_lib.qcuDslash(self._h, _ptr(out), _ptr(inp), int(parity), int(clover), int(precision)))
+
+    def matpc(self, out, inp, kappa: float, clover: bool = False):
+        _check(_lib.qcuMatPC(self._h, _ptr(out), _ptr(inp), float(kappa), int(clover)))
+
+    def mat(self, out, inp, kappa: float, clover: bool = False):
+        _check(_lib.qcuMat(self._h, _ptr(out), _ptr(inp), float(kappa), int(clover)))
+
+    def invert(self, x, b, kappa: float, tol: float = 1e-10, maxiter: int = 10000, precision: int = 64,
+               delta: float = 0.1, clover: bool = False, x0_mode: int = 0, x0_seed: int = 0, abs_tol: bool = False,
+               chunk: int = 0) -> dict:
+        p = QcuInvertParam()
+        _lib.qcuInvertParamDefault(ctypes.byref(p))
+        p.kappa, p.tol, p.maxiter, p.precision, p.delta = kappa, tol, maxiter, precision, delta
+        p.abs_tol, p.x0_mode, p.x0_seed, p.use_clover, p.chunk = int(abs_tol), x0_mode, x0_seed, int(clover), chunk
+        r = QcuInvertResult()
+        _check(_lib.qcuInvert(self._h, _ptr(x), _ptr(b), ctypes.byref(p), ctypes.byref(r)))
+        return r.as_dict()
+
+    def bench_dslash(self, precision: int = 64, clover: bool = False, iters: int = 20) -> float:
+        ms = ctypes.c_double(0)
+        _check(_lib.qcuBenchDslash(self._h, int(precision), int(clover), int(iters), ctypes.byref(ms)))
+        return ms.value
+
+
+def gauge_random(gauge, latt, kind: int = 0, eps: float = 0.25, seed: int = 0):
+    """Fill a PyQuda-layout complex128 gauge buffer: kind 0 Haar, 1 exp(i eps H), 2 unit."""
+    _check(_lib.qcuGaugeRandom(_ptr(gauge), _latt(latt), int(kind), float(eps), int(seed)))
+
+
+def fermion_random(psi, n_complex: int, kind: int = 0, seed: int = 0):
+    """Fill n complex128 values: kind 0 complex normal N(0,1), 1 uniform (0,1]."""
+    _check(_lib.qcuFermionRandom(_ptr(psi), int(n_complex), int(kind), int(seed)))
+
+
+def kernel_launches() -> int:
+    """Kernels launched by libqcu so far in this process (graph replays count every node)."""
+    return int(_lib.qcuKernelLaunches())
+
+
+def stream_handle() -> int:
+    return int(_lib.qcuGetStream() or 0)
+
+
+@dataclass(frozen=True)
+class Layout:
+    """PyQuda field shapes for a lattice [Lx, Ly, Lz, Lt] (field.py:72,78)."""
+
+    latt: tuple
+
+    @property
+    def half(self):
+        Lx, Ly, Lz, Lt = self.latt
+        return (Lt, Lz, Ly, Lx // 2, 4, 3)
+
+    @property
+    def full(self):
+        return (2,) + self.half
+
+    @property
+    def gauge(self):
+        Lx, Ly, Lz, Lt = self.latt
+        return (4, 2, Lt, Lz, Ly, Lx // 2, 3, 3)
+
+    @property
+    def vh(self):
+        Lx, Ly, Lz, Lt = self.latt
+        return Lx * Ly * Lz * Lt // 2

@@ -1,0 +1,277 @@
+// The C ABI: qcu.h (drop-in) and qcu_ext.h (extension).  Every entry point
+// catches internal exceptions and turns them into a recorded last error.
+#include <cstring>
+
+#include "solver.h"
+
+// the library is built with hidden visibility; only the C ABI is exported
+#pragma GCC visibility push(default)
+#include "../../include/qcu.h"
+#include "../../include/qcu_ext.h"
+#pragma GCC visibility pop
+
+namespace qcu {
+int last_error(char *buf, int len);
+}
+
+using namespace qcu;
+
+struct qcuGauge_s {
+  GaugeHandle *h;
+};
+
+#define QCU_API_BEGIN \
+  clear_last_error(); \
+  try {
+#define QCU_API_END                                \
+  return 0;                                        \
+  }                                                \
+  catch (const qcu::Error &e) {                    \
+    set_last_error(e.code, e.what());              \
+    return e.code;                                 \
+  }                                                \
+  catch (const std::exception &e) {                \
+    set_last_error(3, e.what());                   \
+    return 3;                                      \
+  }                                                \
+  catch (...) {                                    \
+    set_last_error(3, "unknown internal error");   \
+    return 3;                                      \
+  }
+
+static void check_grid(const QcuParam *grid) {
+  require(grid != nullptr, "grid pointer is null");
+  for (int d = 0; d < 4; d++)
+    require(grid->lattice_size[d] == 1,
+            "this implementation runs on one GPU: grid must be {1,1,1,1}");
+}
+
+static int legacy_dslash_call(void *out, void *in, void *gauge, QcuParam *param, int parity, int clover) {
+  QCU_API_BEGIN
+  require(param != nullptr, "param pointer is null");
+  legacy_dslash(out, in, gauge, param->lattice_size, parity, clover);
+  QCU_API_END
+}
+
+extern "C" {
+
+// ---------------------------------------------------------------- qcu.h
+void dslashQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, int parity) {
+  legacy_dslash_call(fermion_out, fermion_in, gauge, param, parity, 0);
+}
+
+void dslashCloverQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, int parity) {
+  legacy_dslash_call(fermion_out, fermion_in, gauge, param, parity, 1);
+}
+
+void mpiDslashQcu(void *, void *, void *, QcuParam *, int, QcuParam *) {}
+void mpiBistabCgQcu(void *, QcuParam *, QcuParam *) {}
+
+void ncclDslashQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, int parity, QcuParam *grid) {
+  clear_last_error();
+  try {
+    check_grid(grid);
+  } catch (const qcu::Error &e) {
+    set_last_error(e.code, e.what());
+    return;
+  }
+  legacy_dslash_call(fermion_out, fermion_in, gauge, param, parity, 0);
+}
+
+void ncclBistabCgQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, QcuParam *grid) {
+  clear_last_error();
+  GaugeHandle *G = nullptr;
+  try {
+    require(param != nullptr, "param pointer is null");
+    check_grid(grid);
+    G = gauge_load(gauge, param->lattice_size, 1.0, 0.0);
+    SolveParams p;
+    p.kappa = 0.125;   // include/define.h:69
+    p.tol = 1e-9;      // include/define.h:68, absolute on ||r||^2
+    p.abs_tol = 1;
+    p.maxiter = 1000;  // include/define.h:67
+    p.precision = 64;
+    p.delta = 0.0;
+    p.x0_mode = 2;     // random start, include/lattice_bistabcg.h:108-109
+    p.x0_seed = 23333;
+    solve(*G, fermion_out, fermion_in, p);
+  } catch (const qcu::Error &e) {
+    set_last_error(e.code, e.what());
+  } catch (const std::exception &e) {
+    set_last_error(3, e.what());
+  }
+  delete G;
+}
+
+// ---------------------------------------------------------------- qcu_ext.h
+int qcuGetLastError(char *msg, int len) { return last_error(msg, len); }
+int qcuVersion(void) { return 1; }
+
+int qcuGaugeLoad(qcuGauge *h, const void *gauge, const int latt[4], double t_boundary, double clover_coeff) {
+  QCU_API_BEGIN
+  require(h != nullptr, "handle pointer is null");
+  *h = nullptr;
+  GaugeHandle *G = gauge_load(gauge, latt, t_boundary, clover_coeff);
+  *h = new qcuGauge_s{G};
+  QCU_API_END
+}
+
+int qcuGaugeFree(qcuGauge h) {
+  QCU_API_BEGIN
+  if (h) {
+    delete h->h;
+    delete h;
+  }
+  QCU_API_END
+}
+
+int qcuDslash(qcuGauge h, void *out, const void *in, int parity, int use_clover, int precision) {
+  QCU_API_BEGIN
+  require(h != nullptr, "null gauge handle");
+  handle_dslash(*h->h, out, in, parity, use_clover, precision);
+  QCU_API_END
+}
+
+int qcuMatPC(qcuGauge h, void *out, const void *in, double kappa, int use_clover) {
+  QCU_API_BEGIN
+  require(h != nullptr, "null gauge handle");
+  handle_mpc(*h->h, out, in, kappa, use_clover);
+  QCU_API_END
+}
+
+int qcuMat(qcuGauge h, void *out, const void *in, double kappa, int use_clover) {
+  QCU_API_BEGIN
+  require(h != nullptr, "null gauge handle");
+  handle_mat(*h->h, out, in, kappa, use_clover);
+  QCU_API_END
+}
+
+void qcuInvertParamDefault(qcuInvertParam *p) {
+  if (!p) return;
+  SolveParams d;
+  p->kappa = d.kappa;
+  p->tol = d.tol;
+  p->maxiter = d.maxiter;
+  p->precision = d.precision;
+  p->delta = d.delta;
+  p->abs_tol = d.abs_tol;
+  p->x0_mode = d.x0_mode;
+  p->x0_seed = d.x0_seed;
+  p->use_clover = d.use_clover;
+  p->chunk = d.chunk;
+}
+
+int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuInvertResult *r) {
+  QCU_API_BEGIN
+  require(h != nullptr && p != nullptr, "null handle or parameter pointer");
+  SolveParams s;
+  s.kappa = p->kappa;
+  s.tol = p->tol;
+  s.maxiter = p->maxiter;
+  s.precision = p->precision;
+  s.delta = p->delta;
+  s.abs_tol = p->abs_tol;
+  s.x0_mode = p->x0_mode;
+  s.x0_seed = p->x0_seed;
+  s.use_clover = p->use_clover;
+  s.chunk = p->chunk;
+  require(s.tol > 0, "tol must be positive");
+  require(s.delta >= 0 && s.delta < 1, "delta must be in [0, 1)");
+  SolveInfo info = solve(*h->h, x, b, s);
+  if (r) {
+    r->iterations = info.iterations;
+    r->reliable_updates = info.updates;
+    r->status = info.status;
+    r->restarts = info.restarts;
+    r->true_residual = info.true_residual;
+    r->iter_residual2 = info.iter_residual2;
+    r->seconds = info.seconds;
+  }
+  QCU_API_END
+}
+
+int qcuGaugeRandom(void *gauge, const int latt[4], int kind, double eps, unsigned long long seed) {
+  QCU_API_BEGIN
+  require(gauge != nullptr, "gauge pointer is null");
+  require(kind >= 0 && kind <= 2, "gauge kind must be 0 (Haar), 1 (smooth) or 2 (unit)");
+  const Geom g = make_geom(latt);
+  Context &ctx = context();
+  QCU_CUDA(cudaDeviceSynchronize());
+  launch_gauge_random(g, gauge, kind, eps, seed, ctx.stream);
+  QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+  QCU_API_END
+}
+
+int qcuFermionRandom(void *psi, long long n, int kind, unsigned long long seed) {
+  QCU_API_BEGIN
+  require(psi != nullptr && n >= 0, "bad fermion buffer");
+  require(kind == 0 || kind == 1, "fermion kind must be 0 (normal) or 1 (uniform)");
+  Context &ctx = context();
+  QCU_CUDA(cudaDeviceSynchronize());
+  if (n > 0) launch_fermion_random(psi, n, kind, seed, ctx.stream);
+  QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+  QCU_API_END
+}
+
+long long qcuKernelLaunches(void) { return launch_count(); }
+
+void *qcuGetStream(void) {
+  try {
+    return (void *)context().stream;
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+int qcuBenchDslash(qcuGauge h, int precision, int use_clover, int iters, double *ms_per_call) {
+  QCU_API_BEGIN
+  require(h != nullptr && ms_per_call != nullptr && iters > 0, "bad arguments");
+  GaugeHandle &G = *h->h;
+  require(!use_clover || G.has_clover, "no clover term loaded");
+  const int kind = precision == 64 ? SOA64 : precision == 32 ? SOA32 : precision == 16 ? SOA16 : -1;
+  require(kind >= 0, "precision must be 64, 32 or 16");
+  Context &ctx = context();
+  std::lock_guard<std::mutex> lk(ctx.mu);
+  const int Vh = G.g.Vh;
+  Spinor a, b;
+  a.alloc(kind, Vh);
+  b.alloc(kind, Vh);
+  DevBuf tmp;
+  tmp.ensure(spinor_bytes(AOS64, Vh));
+  launch_fermion_random(tmp.p, (int64_t)Vh * 12, 0, 12345, ctx.stream);
+  launch_convert(AOS64, kind, Vh, tmp.p, nullptr, a.data.p, a.norm.as<float>(), ctx.stream);
+  launch_convert(AOS64, kind, Vh, tmp.p, nullptr, b.data.p, b.norm.as<float>(), ctx.stream);
+  DslashArgs d;
+  d.gauge = G.gauge(kind);
+  d.t_bc = G.t_bc;
+  d.a = 1.0;
+  auto run = [&](int i) {
+    const int par = i & 1;
+    const Spinor &in = par ? a : b;
+    Spinor &out = par ? b : a;
+    d.in = in.data.p;
+    d.in_norm = in.norm.as<float>();
+    d.out = out.data.p;
+    d.out_norm = out.norm.as<float>();
+    d.parity = par;
+    d.clover = use_clover ? G.clover_inv(kind, par) : nullptr;
+    launch_dslash(kind, kind == SOA64 ? GSOA64 : kind == SOA32 ? GSOA32 : GSOA16, kind == SOA64 ? CSOA64 : CSOA32,
+                  G.g, d, ctx, ctx.stream);
+  };
+  for (int i = 0; i < 3; i++) run(i);
+  cudaEvent_t e0, e1;
+  QCU_CUDA(cudaEventCreate(&e0));
+  QCU_CUDA(cudaEventCreate(&e1));
+  QCU_CUDA(cudaEventRecord(e0, ctx.stream));
+  for (int i = 0; i < iters; i++) run(i);
+  QCU_CUDA(cudaEventRecord(e1, ctx.stream));
+  QCU_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  QCU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms_per_call = (double)ms / iters;
+  QCU_API_END
+}
+
+}  // extern "C"

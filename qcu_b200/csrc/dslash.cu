@@ -1,0 +1,123 @@
+// Wilson / clover hopping-term kernels for sm_100a.
+//
+// One thread per output site of one parity; the eight neighbour spinors and
+// eight reconstruct-12 links are read with 16-byte (8-byte for FP16 links)
+// read-only loads in component-major layouts, so every warp instruction moves
+// contiguous 256-512 byte segments and neighbour re-reads hit L1/L2.  The
+// epilogue fuses, in registers, what the solver would otherwise do in extra
+// passes over HBM:
+//     w   = D_{p<-1-p} in                      (qcu's wilson_dslash, src/wilson_dslash.cu:9-245)
+//     w   = A_p^{-1} w          (clover)       (qcu's give_clover, src/clover_dslash.cu:857-882)
+//     out = a*w + b1*x1 + b2*x2                (qcu's bistabcg_give_dest_o/_b__0, src/bistabcg.cu:73-96)
+//     and one of  <rt, out>,  <out, x1> & |out|^2,  |out|^2  reduced to the solver state.
+#include "internal.h"
+
+namespace qcu {
+
+template <int K, int G, int C, bool CLOV, int NX, int RED>
+__global__ void __launch_bounds__(DSLASH_BLOCK) k_dslash(Geom g, DslashArgs a, RedCtx rc) {
+  using T = typename SpinorReal<K>::T;
+  if (!gate_open(rc.st, a.gate)) return;
+  constexpr int NV = RED == RED_NONE ? 1 : (RED == RED_TS_TT ? 3 : (RED == RED_DOT_RT ? 2 : 1));
+  double red[NV];
+#pragma unroll
+  for (int k = 0; k < NV; k++) red[k] = 0.0;
+  const int s = blockIdx.x * DSLASH_BLOCK + threadIdx.x;
+  if (s < g.Vh) {
+    Cpx<T> w[12];
+    const SpinorView<K> in{const_cast<void *>(a.in), const_cast<float *>(a.in_norm), g.Vh};
+    const GaugeView<G> U{a.gauge, g.Vh};
+    wilson_hop_site<K, G, T>(w, in, U, g, s, a.parity, (T)a.t_bc);
+    if constexpr (CLOV) clover_apply_site<C, T>(CloverView<C>{a.clover, g.Vh}, s, w);
+    const T aa = (T)a.a;
+#pragma unroll
+    for (int c = 0; c < 12; c++) w[c] = w[c] * aa;
+    Cpx<T> x1[12];
+    if constexpr (NX >= 1) {
+      spinor_load<K, T>(SpinorView<K>{const_cast<void *>(a.x1), const_cast<float *>(a.x1_norm), g.Vh}, s, x1);
+      const T b1 = (T)a.b1;
+#pragma unroll
+      for (int c = 0; c < 12; c++) w[c] += x1[c] * b1;
+    }
+    if constexpr (NX >= 2) {
+      Cpx<T> x2[12];
+      spinor_load<K, T>(SpinorView<K>{const_cast<void *>(a.x2), const_cast<float *>(a.x2_norm), g.Vh}, s, x2);
+      const T b2 = (T)a.b2;
+#pragma unroll
+      for (int c = 0; c < 12; c++) w[c] += x2[c] * b2;
+    }
+    spinor_store<K, T>(SpinorView<K>{a.out, a.out_norm, g.Vh}, s, w);
+    if constexpr (RED == RED_DOT_RT) {
+      Cpx<T> rt[12];
+      spinor_load<K, T>(SpinorView<K>{const_cast<void *>(a.rt), const_cast<float *>(a.rt_norm), g.Vh}, s, rt);
+#pragma unroll
+      for (int c = 0; c < 12; c++) {
+        red[0] += (double)rt[c].re * (double)w[c].re + (double)rt[c].im * (double)w[c].im;
+        red[1] += (double)rt[c].re * (double)w[c].im - (double)rt[c].im * (double)w[c].re;
+      }
+    } else if constexpr (RED == RED_TS_TT) {
+#pragma unroll
+      for (int c = 0; c < 12; c++) {
+        red[0] += (double)w[c].re * (double)x1[c].re + (double)w[c].im * (double)x1[c].im;
+        red[1] += (double)w[c].re * (double)x1[c].im - (double)w[c].im * (double)x1[c].re;
+        red[2] += (double)w[c].re * (double)w[c].re + (double)w[c].im * (double)w[c].im;
+      }
+    } else if constexpr (RED == RED_NORM) {
+#pragma unroll
+      for (int c = 0; c < 12; c++) red[0] += (double)w[c].re * (double)w[c].re + (double)w[c].im * (double)w[c].im;
+    }
+  }
+  if constexpr (RED != RED_NONE) grid_reduce<NV, DSLASH_BLOCK>(red, rc);
+}
+
+template <int K, int G, int C, bool CLOV, int NX, int RED>
+static void launch_t(const Geom &g, const DslashArgs &a, Context &ctx, cudaStream_t s) {
+  const int blocks = (g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK;
+  RedCtx rc{ctx.st, ctx.partials, a.fin};
+  if (RED != RED_NONE) {
+    require(a.gate == GATE_ALWAYS || ctx.st != nullptr, "reduction without solver state");
+    ctx.ensure_partials(blocks);
+    rc.partials = ctx.partials;
+  }
+  k_dslash<K, G, C, CLOV, NX, RED><<<blocks, DSLASH_BLOCK, 0, s>>>(g, a, rc);
+  QCU_CHECK_LAUNCH();
+}
+
+template <int K, int G, int C, bool CLOV>
+static void launch_nx(const Geom &g, const DslashArgs &a, Context &ctx, cudaStream_t s) {
+  const int nx = a.x2 ? 2 : (a.x1 ? 1 : 0);
+  if (nx == 0) {
+    require(a.red == RED_NONE, "dslash: reduction needs an epilogue source");
+    launch_t<K, G, C, CLOV, 0, RED_NONE>(g, a, ctx, s);
+  } else if (nx == 1) {
+    switch (a.red) {
+      case RED_NONE: launch_t<K, G, C, CLOV, 1, RED_NONE>(g, a, ctx, s); break;
+      case RED_DOT_RT: launch_t<K, G, C, CLOV, 1, RED_DOT_RT>(g, a, ctx, s); break;
+      case RED_TS_TT: launch_t<K, G, C, CLOV, 1, RED_TS_TT>(g, a, ctx, s); break;
+      default: throw Error(1, "dslash: unsupported reduction with one source");
+    }
+  } else {
+    switch (a.red) {
+      case RED_NONE: launch_t<K, G, C, CLOV, 2, RED_NONE>(g, a, ctx, s); break;
+      case RED_NORM: launch_t<K, G, C, CLOV, 2, RED_NORM>(g, a, ctx, s); break;
+      default: throw Error(1, "dslash: unsupported reduction with two sources");
+    }
+  }
+}
+
+template <int K, int G, int C>
+static void launch_clov(const Geom &g, const DslashArgs &a, Context &ctx, cudaStream_t s) {
+  if (a.clover) launch_nx<K, G, C, true>(g, a, ctx, s);
+  else launch_nx<K, G, C, false>(g, a, ctx, s);
+}
+
+void launch_dslash(int kind, int gkind, int ckind, const Geom &g, const DslashArgs &a, Context &ctx,
+                   cudaStream_t s) {
+  if (kind == AOS64 && gkind == GAOS64 && ckind == CSOA64) launch_clov<AOS64, GAOS64, CSOA64>(g, a, ctx, s);
+  else if (kind == SOA64 && gkind == GSOA64 && ckind == CSOA64) launch_clov<SOA64, GSOA64, CSOA64>(g, a, ctx, s);
+  else if (kind == SOA32 && gkind == GSOA32 && ckind == CSOA32) launch_clov<SOA32, GSOA32, CSOA32>(g, a, ctx, s);
+  else if (kind == SOA16 && gkind == GSOA16 && ckind == CSOA32) launch_clov<SOA16, GSOA16, CSOA32>(g, a, ctx, s);
+  else throw Error(1, "dslash: unsupported storage combination");
+}
+
+}  // namespace qcu

@@ -1,0 +1,354 @@
+// Device-side views of the lattice fields and the Wilson stencil core.
+//
+// Storage kinds (one parity, Vh sites, `stride` elements per component):
+//   AOS64 : PyQuda's own layout, complex128 [site][spin*3+colour]
+//           (python/PyQuda/pyquda/field.py:78,230) -- used by the legacy ABI
+//           so a single dslash needs no layout conversion at all.
+//   SOA64 : double2 [12][stride]    component-major, one 16-byte load per
+//           component, 512 contiguous bytes per warp instruction.
+//   SOA32 : float4  [6][stride]     two complex components per 16-byte load.
+//   SOA16 : uint4   [3][stride] + float norm[stride]   FP16 values scaled by
+//           the per-site max |component| (four complex per 16-byte load).
+// Gauge kinds (reconstruct-12: rows 0 and 1 stored, row 2 = conj(r0 x r1),
+// include/define.h:198-206):
+//   GAOS64 : PyQuda layout complex128 [dir][par][site][3][3], rows 0-1 read
+//   GSOA64 : double2 [dir][par][6][stride]
+//   GSOA32 : float4  [dir][par][3][stride]
+//   GSOA16 : uint2   [dir][par][3][stride]   (four FP16 per load, |U_ij| <= 1)
+#pragma once
+#include "cplx.cuh"
+
+namespace qcu {
+
+enum SpinorKind { AOS64 = 0, SOA64 = 1, SOA32 = 2, SOA16 = 3 };
+enum GaugeKind { GAOS64 = 0, GSOA64 = 1, GSOA32 = 2, GSOA16 = 3 };
+
+template <int K> struct SpinorReal { using T = float; };
+template <> struct SpinorReal<AOS64> { using T = double; };
+template <> struct SpinorReal<SOA64> { using T = double; };
+
+// Lattice geometry of one parity (half lattice).  Site index
+// i = ((t*Lz + z)*Ly + y)*Lxh + xh, the PyQuda/qcu ordering.
+struct Geom {
+  int Lxh, Ly, Lz, Lt;
+  int sy, sz, st;  // index strides of y, z, t
+  int Vh;
+};
+
+// ------------------------------------------------------------------ spinors
+template <int K>
+struct SpinorView {
+  void *p;
+  float *norm;  // SOA16 only
+  int stride;
+};
+
+template <int K, typename T>
+__device__ __forceinline__ void spinor_load(const SpinorView<K> &v, int s, Cpx<T> out[12]) {
+  if constexpr (K == AOS64) {
+    const double2 *p = static_cast<const double2 *>(v.p) + (size_t)s * 12;
+#pragma unroll
+    for (int c = 0; c < 12; c++) {
+      double2 d = __ldg(p + c);
+      out[c] = Cpx<T>((T)d.x, (T)d.y);
+    }
+  } else if constexpr (K == SOA64) {
+    const double2 *p = static_cast<const double2 *>(v.p) + s;
+#pragma unroll
+    for (int c = 0; c < 12; c++) {
+      double2 d = __ldg(p + (size_t)c * v.stride);
+      out[c] = Cpx<T>((T)d.x, (T)d.y);
+    }
+  } else if constexpr (K == SOA32) {
+    const float4 *p = static_cast<const float4 *>(v.p) + s;
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+      float4 d = __ldg(p + (size_t)c * v.stride);
+      out[2 * c] = Cpx<T>((T)d.x, (T)d.y);
+      out[2 * c + 1] = Cpx<T>((T)d.z, (T)d.w);
+    }
+  } else {
+    const uint4 *p = static_cast<const uint4 *>(v.p) + s;
+    float nrm = __ldg(v.norm + s);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      uint4 d = __ldg(p + (size_t)c * v.stride);
+      unsigned w[4] = {d.x, d.y, d.z, d.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        __half2 h = *reinterpret_cast<__half2 *>(&w[k]);
+        float2 f = __half22float2(h);
+        out[4 * c + k] = Cpx<T>((T)(f.x * nrm), (T)(f.y * nrm));
+      }
+    }
+  }
+}
+
+template <int K, typename T>
+__device__ __forceinline__ void spinor_store(const SpinorView<K> &v, int s, const Cpx<T> in[12]) {
+  if constexpr (K == AOS64) {
+    double2 *p = static_cast<double2 *>(v.p) + (size_t)s * 12;
+#pragma unroll
+    for (int c = 0; c < 12; c++) p[c] = make_double2((double)in[c].re, (double)in[c].im);
+  } else if constexpr (K == SOA64) {
+    double2 *p = static_cast<double2 *>(v.p) + s;
+#pragma unroll
+    for (int c = 0; c < 12; c++) p[(size_t)c * v.stride] = make_double2((double)in[c].re, (double)in[c].im);
+  } else if constexpr (K == SOA32) {
+    float4 *p = static_cast<float4 *>(v.p) + s;
+#pragma unroll
+    for (int c = 0; c < 6; c++)
+      p[(size_t)c * v.stride] = make_float4((float)in[2 * c].re, (float)in[2 * c].im, (float)in[2 * c + 1].re,
+                                            (float)in[2 * c + 1].im);
+  } else {
+    float mx = 0.f;
+#pragma unroll
+    for (int c = 0; c < 12; c++) mx = fmaxf(mx, fmaxf(fabsf((float)in[c].re), fabsf((float)in[c].im)));
+    float inv = mx > 0.f ? 1.0f / mx : 0.f;
+    uint4 *p = static_cast<uint4 *>(v.p) + s;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      unsigned w[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        __half2 h = __floats2half2_rn((float)in[4 * c + k].re * inv, (float)in[4 * c + k].im * inv);
+        w[k] = *reinterpret_cast<unsigned *>(&h);
+      }
+      p[(size_t)c * v.stride] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    v.norm[s] = mx;
+  }
+}
+
+// ------------------------------------------------------------------ gauge
+template <int G>
+struct GaugeView {
+  const void *p;
+  int stride;  // sites per (dir, parity) slab (= Vh)
+};
+
+// rows 0 and 1 of U_dir(site) on parity par, then row 2 = conj(row0 x row1)
+template <int G, typename T>
+__device__ __forceinline__ void link_load(const GaugeView<G> &u, int dir, int par, int s, Cpx<T> m[9]) {
+  const size_t slab = (size_t)(dir * 2 + par) * u.stride;
+  if constexpr (G == GAOS64) {
+    const double2 *p = static_cast<const double2 *>(u.p) + (slab + s) * 9;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      double2 d = __ldg(p + k);
+      m[k] = Cpx<T>((T)d.x, (T)d.y);
+    }
+  } else if constexpr (G == GSOA64) {
+    const double2 *p = static_cast<const double2 *>(u.p) + slab * 6 + s;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      double2 d = __ldg(p + (size_t)k * u.stride);
+      m[k] = Cpx<T>((T)d.x, (T)d.y);
+    }
+  } else if constexpr (G == GSOA32) {
+    const float4 *p = static_cast<const float4 *>(u.p) + slab * 3 + s;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      float4 d = __ldg(p + (size_t)k * u.stride);
+      m[2 * k] = Cpx<T>((T)d.x, (T)d.y);
+      m[2 * k + 1] = Cpx<T>((T)d.z, (T)d.w);
+    }
+  } else {
+    const uint2 *p = static_cast<const uint2 *>(u.p) + slab * 3 + s;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      uint2 d = __ldg(p + (size_t)k * u.stride);
+      unsigned w[2] = {d.x, d.y};
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        float2 f = __half22float2(*reinterpret_cast<__half2 *>(&w[q]));
+        m[2 * k + q] = Cpx<T>((T)f.x, (T)f.y);
+      }
+    }
+  }
+  m[6] = (m[1] * m[5] - m[2] * m[4]).conj();
+  m[7] = (m[2] * m[3] - m[0] * m[5]).conj();
+  m[8] = (m[0] * m[4] - m[1] * m[3]).conj();
+}
+
+// ------------------------------------------------------------------ stencil
+// DeGrand-Rossi gamma matrices: row r of gamma_mu has one non-zero entry, in
+// column GCOL[mu][r], with value GRE + i*GIM.  These are the projections qcu
+// hard-codes in src/wilson_dslash.cu:56-243.
+__host__ __device__ constexpr int gcol(int mu, int r) {
+  return (mu < 2) ? (3 - r) : ((r + 2) & 3);
+}
+__host__ __device__ constexpr int gre(int mu, int r) {
+  return mu == 1 ? ((r == 0 || r == 3) ? -1 : 1) : (mu == 3 ? 1 : 0);
+}
+__host__ __device__ constexpr int gim(int mu, int r) {
+  return mu == 0 ? (r < 2 ? 1 : -1) : (mu == 2 ? ((r == 0 || r == 3) ? 1 : -1) : 0);
+}
+
+// acc += U (1 - gamma_mu) psi   (FWD)   or   acc += U^dag (1 + gamma_mu) psi   (!FWD)
+// The projector has rank 2: rows 0,1 give h_k = psi_k + sigma*g_k*psi_col(k);
+// rows 2,3 are sigma*g_m * h_col(m).
+template <int MU, bool FWD, typename T>
+__device__ __forceinline__ void hop(Cpx<T> acc[12], const Cpx<T> psi[12], const Cpx<T> u[9], T phase) {
+  constexpr int S = FWD ? -1 : 1;
+  Cpx<T> h[2][3], uh[2][3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    h[0][c] = psi[c] + unit_mul<S * gre(MU, 0), S * gim(MU, 0)>(psi[gcol(MU, 0) * 3 + c]);
+    h[1][c] = psi[3 + c] + unit_mul<S * gre(MU, 1), S * gim(MU, 1)>(psi[gcol(MU, 1) * 3 + c]);
+  }
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      Cpx<T> s;
+      if constexpr (FWD) {
+        s = u[r * 3 + 0] * h[k][0];
+        s += u[r * 3 + 1] * h[k][1];
+        s += u[r * 3 + 2] * h[k][2];
+      } else {
+        s = cdotmul(u[0 * 3 + r], h[k][0]);
+        s += cdotmul(u[1 * 3 + r], h[k][1]);
+        s += cdotmul(u[2 * 3 + r], h[k][2]);
+      }
+      if constexpr (MU == 3) s = s * phase;
+      uh[k][r] = s;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    acc[c] += uh[0][c];
+    acc[3 + c] += uh[1][c];
+    acc[6 + c] += unit_mul<S * gre(MU, 2), S * gim(MU, 2)>(uh[gcol(MU, 2)][c]);
+    acc[9 + c] += unit_mul<S * gre(MU, 3), S * gim(MU, 3)>(uh[gcol(MU, 3)][c]);
+  }
+}
+
+// Hopping term D_{p <- 1-p} at output site s of parity `par`:
+//   sum_mu U_mu(x)(1-g_mu) in(x+mu) + U_mu(x-mu)^+ (1+g_mu) in(x-mu)
+// periodic in x,y,z; t-boundary hops multiplied by t_bc.
+template <int K, int G, typename T>
+__device__ __forceinline__ void wilson_hop_site(Cpx<T> acc[12], const SpinorView<K> &in, const GaugeView<G> &U,
+                                                const Geom &g, int s, int par, T t_bc) {
+#pragma unroll
+  for (int c = 0; c < 12; c++) acc[c] = Cpx<T>(0, 0);
+  const int xh = s % g.Lxh;
+  int r = s / g.Lxh;
+  const int y = r % g.Ly;
+  r /= g.Ly;
+  const int z = r % g.Lz;
+  const int t = r / g.Lz;
+  const int xodd = (y + z + t + par) & 1;  // full x = 2*xh + xodd
+  Cpx<T> psi[12], u[9];
+  int n;
+  // x
+  n = xodd ? (xh == g.Lxh - 1 ? s - xh : s + 1) : s;
+  spinor_load<K, T>(in, n, psi);
+  link_load<G, T>(U, 0, par, s, u);
+  hop<0, true, T>(acc, psi, u, T(1));
+  n = xodd ? s : (xh == 0 ? s + g.Lxh - 1 : s - 1);
+  spinor_load<K, T>(in, n, psi);
+  link_load<G, T>(U, 0, 1 - par, n, u);
+  hop<0, false, T>(acc, psi, u, T(1));
+  // y
+  n = (y == g.Ly - 1) ? s - (g.Ly - 1) * g.sy : s + g.sy;
+  spinor_load<K, T>(in, n, psi);
+  link_load<G, T>(U, 1, par, s, u);
+  hop<1, true, T>(acc, psi, u, T(1));
+  n = (y == 0) ? s + (g.Ly - 1) * g.sy : s - g.sy;
+  spinor_load<K, T>(in, n, psi);
+  link_load<G, T>(U, 1, 1 - par, n, u);
+  hop<1, false, T>(acc, psi, u, T(1));
+  // z
+  n = (z == g.Lz - 1) ? s - (g.Lz - 1) * g.sz : s + g.sz;
+  spinor_load<K, T>(in, n, psi);
+  link_load<G, T>(U, 2, par, s, u);
+  hop<2, true, T>(acc, psi, u, T(1));
+  n = (z == 0) ? s + (g.Lz - 1) * g.sz : s - g.sz;
+  spinor_load<K, T>(in, n, psi);
+  link_load<G, T>(U, 2, 1 - par, n, u);
+  hop<2, false, T>(acc, psi, u, T(1));
+  // t
+  n = (t == g.Lt - 1) ? s - (g.Lt - 1) * g.st : s + g.st;
+  spinor_load<K, T>(in, n, psi);
+  link_load<G, T>(U, 3, par, s, u);
+  hop<3, true, T>(acc, psi, u, (t == g.Lt - 1) ? t_bc : T(1));
+  n = (t == 0) ? s + (g.Lt - 1) * g.st : s - g.st;
+  spinor_load<K, T>(in, n, psi);
+  link_load<G, T>(U, 3, 1 - par, n, u);
+  hop<3, false, T>(acc, psi, u, (t == 0) ? t_bc : T(1));
+}
+
+// ------------------------------------------------------------------ clover
+// Packed clover (or inverse clover) per site: two Hermitian 6x6 chiral blocks
+// (spins {0,1} and {2,3} in the DeGrand-Rossi basis), each 36 reals:
+//   d[0..5] real diagonal, then L[i][j] (i>j) complex at i(i-1)/2 + j.
+// CSOA64: double2 [2][18][stride]   (diag packed as 3 double2, then 15)
+// CSOA32: float4  [2][9][stride]
+enum CloverKind { CSOA64 = 0, CSOA32 = 1 };
+template <int C>
+struct CloverView {
+  const void *p;
+  int stride;
+};
+
+template <int C, typename T>
+__device__ __forceinline__ void clover_block_load(const CloverView<C> &cv, int blk, int s, T d[6], Cpx<T> L[15]) {
+  if constexpr (C == CSOA64) {
+    const double2 *p = static_cast<const double2 *>(cv.p) + (size_t)blk * 18 * cv.stride + s;
+    double2 q[18];
+#pragma unroll
+    for (int k = 0; k < 18; k++) q[k] = __ldg(p + (size_t)k * cv.stride);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      d[2 * k] = (T)q[k].x;
+      d[2 * k + 1] = (T)q[k].y;
+    }
+#pragma unroll
+    for (int k = 0; k < 15; k++) L[k] = Cpx<T>((T)q[3 + k].x, (T)q[3 + k].y);
+  } else {
+    const float4 *p = static_cast<const float4 *>(cv.p) + (size_t)blk * 9 * cv.stride + s;
+    float f[36];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      float4 q = __ldg(p + (size_t)k * cv.stride);
+      f[4 * k] = q.x;
+      f[4 * k + 1] = q.y;
+      f[4 * k + 2] = q.z;
+      f[4 * k + 3] = q.w;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; k++) d[k] = (T)f[k];
+#pragma unroll
+    for (int k = 0; k < 15; k++) L[k] = Cpx<T>((T)f[6 + 2 * k], (T)f[7 + 2 * k]);
+  }
+}
+
+// v <- C v for both chiral blocks of one site
+template <int C, typename T>
+__device__ __forceinline__ void clover_apply_site(const CloverView<C> &cv, int s, Cpx<T> v[12]) {
+#pragma unroll
+  for (int blk = 0; blk < 2; blk++) {
+    T d[6];
+    Cpx<T> L[15];
+    clover_block_load<C, T>(cv, blk, s, d, L);
+    Cpx<T> x[6], y[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) x[i] = v[blk * 6 + i];
+#pragma unroll
+    for (int i = 0; i < 6; i++) y[i] = x[i] * d[i];
+#pragma unroll
+    for (int i = 1; i < 6; i++) {
+#pragma unroll
+      for (int j = 0; j < i; j++) {
+        const Cpx<T> l = L[i * (i - 1) / 2 + j];
+        y[i] += l * x[j];
+        y[j] += cdotmul(l, x[i]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 6; i++) v[blk * 6 + i] = y[i];
+  }
+}
+
+}  // namespace qcu

@@ -1,0 +1,121 @@
+// Runtime support: error recording, device buffers, the per-device context.
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <memory>
+
+#include "internal.h"
+
+namespace qcu {
+
+// ---------------------------------------------------------------- errors
+static thread_local int g_err_code = 0;
+static thread_local std::string g_err_msg;
+
+void set_last_error(int code, const std::string &msg) {
+  g_err_code = code;
+  g_err_msg = msg;
+  if (getenv("QCU_QUIET") == nullptr) fprintf(stderr, "qcu: %s\n", msg.c_str());
+}
+void clear_last_error() {
+  g_err_code = 0;
+  g_err_msg.clear();
+}
+int last_error(char *buf, int len) {
+  if (buf && len > 0) {
+    strncpy(buf, g_err_msg.c_str(), (size_t)len - 1);
+    buf[len - 1] = 0;
+  }
+  return g_err_code;
+}
+
+// ---------------------------------------------------------------- launch counter
+static std::atomic<long long> g_launches{0};
+void note_launch(long long n) { g_launches += n; }
+long long launch_count() { return g_launches.load(); }
+void set_launch_count(long long v) { g_launches = v; }
+
+// ---------------------------------------------------------------- geometry
+Geom make_geom(const int latt[4]) {
+  require(latt != nullptr, "lattice size pointer is null");
+  for (int d = 0; d < 4; d++) require(latt[d] > 0, "lattice sizes must be positive");
+  require(latt[0] % 2 == 0, "Lx must be even for the even-odd layout");
+  const int64_t vh = (int64_t)latt[0] / 2 * latt[1] * latt[2] * latt[3];
+  require(vh < (1LL << 28), "lattice too large (Vh must be < 2^28)");
+  Geom g;
+  g.Lxh = latt[0] / 2;
+  g.Ly = latt[1];
+  g.Lz = latt[2];
+  g.Lt = latt[3];
+  g.sy = g.Lxh;
+  g.sz = g.Lxh * g.Ly;
+  g.st = g.Lxh * g.Ly * g.Lz;
+  g.Vh = (int)vh;
+  return g;
+}
+
+size_t spinor_bytes(int kind, int Vh) {
+  switch (kind) {
+    case AOS64:
+    case SOA64: return (size_t)Vh * 12 * 16;
+    case SOA32: return (size_t)Vh * 12 * 8;
+    case SOA16: return (size_t)Vh * 12 * 4;
+  }
+  return 0;
+}
+size_t spinor_norm_bytes(int kind, int Vh) { return kind == SOA16 ? (size_t)Vh * 4 : 0; }
+
+// ---------------------------------------------------------------- buffers
+DevBuf::~DevBuf() { release(); }
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  n = 0;
+}
+void DevBuf::ensure(size_t bytes) {
+  if (bytes <= n) return;
+  release();
+  if (bytes == 0) return;
+  QCU_CUDA(cudaMalloc(&p, bytes));
+  n = bytes;
+}
+
+void Spinor::alloc(int k, int vh) {
+  kind = k;
+  Vh = vh;
+  data.ensure(spinor_bytes(k, vh));
+  if (k == SOA16) norm.ensure(spinor_norm_bytes(k, vh));
+}
+
+// ---------------------------------------------------------------- context
+void Context::ensure_partials(size_t blocks) {
+  if (blocks <= partials_blocks) return;
+  if (partials) cudaFree(partials);
+  partials = nullptr;
+  QCU_CUDA(cudaMalloc(&partials, blocks * 8 * sizeof(double)));
+  partials_blocks = blocks;
+}
+
+static std::mutex g_ctx_mu;
+static std::map<int, std::unique_ptr<Context>> g_ctx;
+
+Context &context() {
+  int dev = 0;
+  QCU_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  auto it = g_ctx.find(dev);
+  if (it != g_ctx.end()) return *it->second;
+  auto c = std::make_unique<Context>();
+  c->device = dev;
+  QCU_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  QCU_CUDA(cudaMalloc(&c->st, sizeof(SolverState)));
+  QCU_CUDA(cudaMemset(c->st, 0, sizeof(SolverState)));
+  QCU_CUDA(cudaMallocHost(&c->st_host, sizeof(SolverState)));
+  memset(c->st_host, 0, sizeof(SolverState));
+  c->ensure_partials(MAX_REDUCE_BLOCKS);
+  Context &ref = *c;
+  g_ctx[dev] = std::move(c);
+  return ref;
+}
+
+}  // namespace qcu

@@ -1,0 +1,424 @@
+// Operator application and the BiCGSTAB driver.
+//
+// The algorithm is qcu's even-odd preconditioned BiCGSTAB
+// (include/lattice_bistabcg.h:101-132,221-340): b'_o = b_o + kappa D_oe b_e,
+// solve (1 - kappa^2 D_oe D_eo) x_o = b'_o, then x_e = b_e + kappa D_eo x_o,
+// extended with the clover term (A_p^-1 applied after each hop) and with an
+// inner precision below FP64 corrected by reliable updates: the FP64 true
+// residual b' - M_pc x64 replaces the iterated one whenever the latter has
+// dropped by `delta`, and always before convergence is declared.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "solver.h"
+
+namespace qcu {
+
+static int kind_of_precision(int prec) {
+  switch (prec) {
+    case 64: return SOA64;
+    case 32: return SOA32;
+    case 16: return SOA16;
+  }
+  throw Error(1, "precision must be 64, 32 or 16");
+}
+static int gkind_of(int kind) { return kind == SOA64 ? GSOA64 : (kind == SOA32 ? GSOA32 : GSOA16); }
+static int ckind_of(int kind) { return kind == SOA64 ? CSOA64 : CSOA32; }
+
+GaugeHandle *gauge_load(const void *gauge_pyq, const int latt[4], double t_bc, double clover_coeff) {
+  require(gauge_pyq != nullptr, "gauge pointer is null");
+  require(t_bc == 1.0 || t_bc == -1.0, "t boundary must be +1 or -1");
+  Context &ctx = context();
+  auto *G = new GaugeHandle();
+  try {
+    for (int d = 0; d < 4; d++) G->latt[d] = latt[d];
+    G->g = make_geom(latt);
+    G->t_bc = t_bc;
+    const int Vh = G->g.Vh;
+    G->g64.ensure(gauge_bytes(GSOA64, Vh));
+    G->g32.ensure(gauge_bytes(GSOA32, Vh));
+    G->g16.ensure(gauge_bytes(GSOA16, Vh));
+    launch_gauge_pack(GSOA64, G->g, gauge_pyq, G->g64.p, ctx.stream);
+    launch_gauge_pack(GSOA32, G->g, gauge_pyq, G->g32.p, ctx.stream);
+    launch_gauge_pack(GSOA16, G->g, gauge_pyq, G->g16.p, ctx.stream);
+    if (clover_coeff != 0.0) {
+      G->has_clover = true;
+      G->clover_coeff = clover_coeff;
+      DevBuf bad;
+      bad.ensure(sizeof(int));
+      QCU_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx.stream));
+      for (int p = 0; p < 2; p++) {
+        G->A64[p].ensure(clover_bytes(CSOA64, Vh));
+        G->Ainv64[p].ensure(clover_bytes(CSOA64, Vh));
+        G->Ainv32[p].ensure(clover_bytes(CSOA32, Vh));
+        launch_clover_build(G->g, gauge_pyq, p, clover_coeff, G->A64[p].p, G->Ainv64[p].p, bad.as<int>(), ctx.stream);
+        launch_clover_to32(Vh, G->Ainv64[p].p, G->Ainv32[p].p, ctx.stream);
+      }
+      int nbad = 0;
+      QCU_CUDA(cudaMemcpyAsync(&nbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+      QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+      require(nbad == 0, "clover term is singular on " + std::to_string(nbad) + " site blocks");
+    }
+    QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+  } catch (...) {
+    delete G;
+    throw;
+  }
+  return G;
+}
+
+// ---------------------------------------------------------------- workspace
+namespace {
+struct Workspace {
+  Spinor be, bo, bp, x64, r64, tmp64, xe, aux;  // FP64
+  Spinor r, rt, p, v, s, t, tmp, x;             // inner precision (x: FP64 or FP32)
+  void prepare(int kind, int Vh) {
+    for (Spinor *q : {&be, &bo, &bp, &x64, &r64, &tmp64, &xe, &aux}) q->alloc(SOA64, Vh);
+    for (Spinor *q : {&r, &rt, &p, &v, &s, &t, &tmp}) q->alloc(kind, Vh);
+    x.alloc(kind == SOA64 ? SOA64 : SOA32, Vh);
+  }
+};
+Workspace &workspace() {
+  static Workspace *w = new Workspace();  // intentionally never destroyed (lives until exit)
+  return *w;
+}
+}  // namespace
+
+struct Dsl {
+  const GaugeHandle &G;
+  Context &ctx;
+  int kind;
+  // out = a * [Ainv_par] D in + b1 x1 + b2 x2 (+ fused reduction)
+  void operator()(int par, const Spinor &in, Spinor &out, bool clover, double a, const Spinor *x1 = nullptr,
+                  double b1 = 0, const Spinor *x2 = nullptr, double b2 = 0, int red = RED_NONE, int fin = FIN_STORE,
+                  const Spinor *rt = nullptr, int gate = GATE_ALWAYS) {
+    DslashArgs d;
+    d.in = in.data.p;
+    d.in_norm = in.norm.as<float>();
+    d.out = out.data.p;
+    d.out_norm = out.norm.as<float>();
+    if (x1) {
+      d.x1 = x1->data.p;
+      d.x1_norm = x1->norm.as<float>();
+      d.b1 = b1;
+    }
+    if (x2) {
+      d.x2 = x2->data.p;
+      d.x2_norm = x2->norm.as<float>();
+      d.b2 = b2;
+    }
+    if (rt) {
+      d.rt = rt->data.p;
+      d.rt_norm = rt->norm.as<float>();
+    }
+    d.gauge = G.gauge(kind);
+    d.clover = clover ? G.clover_inv(kind, par) : nullptr;
+    d.parity = par;
+    d.t_bc = G.t_bc;
+    d.a = a;
+    d.red = red;
+    d.fin = fin;
+    d.gate = gate;
+    launch_dslash(kind, gkind_of(kind), ckind_of(kind), G.g, d, ctx, ctx.stream);
+  }
+};
+
+static VecSet make_vecset(Workspace &w) {
+  VecSet vs;
+  vs.r = w.r.data.p;
+  vs.rn = w.r.norm.as<float>();
+  vs.rt = w.rt.data.p;
+  vs.rtn = w.rt.norm.as<float>();
+  vs.p = w.p.data.p;
+  vs.pn = w.p.norm.as<float>();
+  vs.v = w.v.data.p;
+  vs.vn = w.v.norm.as<float>();
+  vs.s = w.s.data.p;
+  vs.sn = w.s.norm.as<float>();
+  vs.t = w.t.data.p;
+  vs.tn = w.t.norm.as<float>();
+  vs.x = w.x.data.p;
+  vs.xn = w.x.norm.as<float>();
+  vs.x64 = w.x64.data.p;
+  vs.r64 = w.r64.data.p;
+  return vs;
+}
+
+static SolverState read_state(Context &ctx) {
+  QCU_CUDA(cudaMemcpyAsync(ctx.st_host, ctx.st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx.stream));
+  QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+  return *ctx.st_host;
+}
+
+static double dots_norm2(Context &ctx, int kind, int Vh, void *a, float *an) {
+  launch_dots(kind, Vh, a, an, a, an, ctx, ctx.stream);
+  return read_state(ctx).sums[2];
+}
+
+// one BiCGSTAB iteration (plus the gated reliable-update sequence)
+static void enqueue_iteration(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, double kappa, bool clov) {
+  Context &ctx = dP.ctx;
+  const int Vh = dP.G.g.Vh, kind = dP.kind;
+  const double k2 = kappa * kappa;
+  launch_pupdate(kind, Vh, vs, ctx.st, GATE_NOT_DONE, ctx.stream);
+  dP(0, w.p, w.tmp, clov, 1.0, nullptr, 0, nullptr, 0, RED_NONE, FIN_STORE, nullptr, GATE_NOT_DONE);
+  dP(1, w.tmp, w.v, clov, -k2, &w.p, 1.0, nullptr, 0, RED_DOT_RT, FIN_ALPHA, &w.rt, GATE_NOT_DONE);
+  launch_supdate(kind, Vh, vs, ctx.st, GATE_NOT_DONE, ctx.stream);
+  dP(0, w.s, w.tmp, clov, 1.0, nullptr, 0, nullptr, 0, RED_NONE, FIN_STORE, nullptr, GATE_NOT_DONE);
+  dP(1, w.tmp, w.t, clov, -k2, &w.s, 1.0, nullptr, 0, RED_TS_TT, FIN_OMEGA, nullptr, GATE_NOT_DONE);
+  launch_xrupdate(kind, Vh, vs, ctx, GATE_NOT_DONE, ctx.stream);
+  // reliable update: x64 += x; r64 = b' - M_pc x64 (FP64); r = r64
+  launch_xfold(w.x.kind, Vh, vs, ctx.st, GATE_UPDATE, ctx.stream);
+  d64(0, w.x64, w.tmp64, clov, 1.0, nullptr, 0, nullptr, 0, RED_NONE, FIN_STORE, nullptr, GATE_UPDATE);
+  d64(1, w.tmp64, w.r64, clov, k2, &w.bp, 1.0, &w.x64, -1.0, RED_NORM, FIN_RTRUE, nullptr, GATE_UPDATE);
+  launch_rconv(kind, Vh, vs, ctx, GATE_UPDATE, ctx.stream);
+}
+
+SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParams &prm) {
+  require(x_pyq != nullptr && b_pyq != nullptr, "solve: null spinor pointer");
+  require(prm.kappa > 0, "solve: kappa must be positive");
+  require(prm.maxiter > 0, "solve: maxiter must be positive");
+  require(!prm.use_clover || G.has_clover, "solve: clover requested but the gauge handle has no clover term");
+  const auto t0 = std::chrono::steady_clock::now();
+  Context &ctx = context();
+  std::lock_guard<std::mutex> lk(ctx.mu);
+  const int kind = kind_of_precision(prm.precision);
+  const int Vh = G.g.Vh;
+  const bool clov = prm.use_clover != 0;
+  const double kappa = prm.kappa;
+  Workspace &w = workspace();
+  w.prepare(kind, Vh);
+  Dsl dP{G, ctx, kind}, d64{G, ctx, SOA64};
+  // reduction partials sized once, before any graph capture bakes the pointer in
+  ctx.ensure_partials((size_t)std::max((Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK, MAX_REDUCE_BLOCKS));
+  const size_t half = spinor_bytes(AOS64, Vh);
+  const char *bp = static_cast<const char *>(b_pyq);
+  char *xp = static_cast<char *>(x_pyq);
+  cudaStream_t st = ctx.stream;
+  QCU_CUDA(cudaDeviceSynchronize());  // inputs written on any stream are complete
+
+  // b_e, b_o -> FP64 internal; b'_o = A_o^-1 (b_o + kappa D_oe A_e^-1 b_e)
+  launch_convert(AOS64, SOA64, Vh, bp, nullptr, w.be.data.p, nullptr, st);
+  launch_convert(AOS64, SOA64, Vh, bp + half, nullptr, w.bo.data.p, nullptr, st);
+  if (clov) {
+    launch_clover_apply(SOA64, Vh, G.Ainv64[0].p, w.be.data.p, w.aux.data.p, st);
+    d64(1, w.aux, w.tmp64, false, kappa, &w.bo, 1.0);
+    launch_clover_apply(SOA64, Vh, G.Ainv64[1].p, w.tmp64.data.p, w.bp.data.p, st);
+  } else {
+    d64(1, w.be, w.bp, false, kappa, &w.bo, 1.0);
+  }
+  const double bb = dots_norm2(ctx, SOA64, Vh, w.be.data.p, nullptr) + dots_norm2(ctx, SOA64, Vh, w.bo.data.p, nullptr);
+  SolveInfo info;
+  if (bb == 0.0) {
+    QCU_CUDA(cudaMemsetAsync(x_pyq, 0, 2 * half, st));
+    QCU_CUDA(cudaStreamSynchronize(st));
+    info.status = ST_CONVERGED;
+    return info;
+  }
+  double tol2 = prm.abs_tol ? prm.tol : prm.tol * prm.tol * bb;
+
+  // initial guess
+  if (prm.x0_mode == 1) launch_convert(AOS64, SOA64, Vh, xp + half, nullptr, w.x64.data.p, nullptr, st);
+  else if (prm.x0_mode == 2) launch_uniform_soa64(Vh, w.x64.data.p, prm.x0_seed, st);
+  else QCU_CUDA(cudaMemsetAsync(w.x64.data.p, 0, spinor_bytes(SOA64, Vh), st));
+
+  const VecSet vs = make_vecset(w);
+  int chunk = prm.chunk > 0 ? prm.chunk : (Vh >= (1 << 18) ? 8 : (Vh >= (1 << 14) ? 16 : 32));
+  const bool use_graph = getenv("QCU_NO_GRAPH") == nullptr;
+  int total_iter = 0, total_updates = 0;
+  SolverState S{};
+  for (int restart = 0;; restart++) {
+    // r64 = b' - M_pc x64
+    d64(0, w.x64, w.tmp64, clov, 1.0);
+    d64(1, w.tmp64, w.r64, clov, kappa * kappa, &w.bp, 1.0, &w.x64, -1.0, RED_NORM, FIN_RTRUE);
+    SolverState init{};
+    init.tol2 = tol2;
+    init.delta2 = prm.delta * prm.delta;
+    init.maxiter = prm.maxiter - total_iter;
+    *ctx.st_host = init;
+    QCU_CUDA(cudaMemcpyAsync(ctx.st, ctx.st_host, sizeof(SolverState), cudaMemcpyHostToDevice, st));
+    launch_init(kind, Vh, vs, ctx, st);
+    S = read_state(ctx);
+    if (!S.done) {
+      cudaGraphExec_t exec = nullptr;
+      long long nodes = 0;
+      if (use_graph) {
+        cudaGraph_t graph;
+        const long long before = launch_count();
+        QCU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+          for (int k = 0; k < chunk; k++) enqueue_iteration(dP, d64, w, vs, kappa, clov);
+        } catch (...) {
+          cudaStreamEndCapture(st, &graph);
+          throw;
+        }
+        QCU_CUDA(cudaStreamEndCapture(st, &graph));
+        nodes = launch_count() - before;  // captured, not run: counted per replay below
+        set_launch_count(before);
+        QCU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        QCU_CUDA(cudaGraphDestroy(graph));
+      }
+      // every iteration advances st->iter, and the iteration that reaches
+      // maxiter sets done, so this loop ends after at most maxiter/chunk + 1
+      // passes; the cap below only guards against a logic error
+      const long long max_passes = (long long)init.maxiter / chunk + 8;
+      for (long long pass = 0;; pass++) {
+        require(pass < max_passes, "solver did not terminate within maxiter (internal error)");
+        if (exec) {
+          QCU_CUDA(cudaGraphLaunch(exec, st));
+          note_launch(nodes);
+        } else
+          for (int k = 0; k < chunk; k++) enqueue_iteration(dP, d64, w, vs, kappa, clov);
+        S = read_state(ctx);
+        if (S.done) break;
+      }
+      if (exec) cudaGraphExecDestroy(exec);
+    }
+    // fold whatever the inner solution still holds
+    launch_xfold(w.x.kind, Vh, vs, ctx.st, GATE_ALWAYS, st);
+    total_iter += S.iter;
+    total_updates += S.nupdates;
+    info.status = S.status;
+    info.iter_residual2 = S.rr;
+    // x_e = A_e^-1 (b_e + kappa D_eo x_o)
+    d64(0, w.x64, w.tmp64, false, kappa, &w.be, 1.0);
+    if (clov) launch_clover_apply(SOA64, Vh, G.Ainv64[0].p, w.tmp64.data.p, w.xe.data.p, st);
+    else launch_convert(SOA64, SOA64, Vh, w.tmp64.data.p, nullptr, w.xe.data.p, nullptr, st);
+    // full-system FP64 true residual: r_p = b_p - A_p x_p + kappa D x_{1-p}
+    double rr = 0;
+    for (int p = 0; p < 2; p++) {
+      Spinor &xp_ = p ? w.x64 : w.xe;
+      Spinor &bpar = p ? w.bo : w.be;
+      const Spinor *ax = &xp_;
+      if (clov) {
+        launch_clover_apply(SOA64, Vh, G.A64[p].p, xp_.data.p, w.aux.data.p, st);
+        ax = &w.aux;
+      }
+      d64(p, p ? w.xe : w.x64, w.tmp64, false, kappa, &bpar, 1.0, ax, -1.0, RED_NORM, FIN_STORE);
+      rr += read_state(ctx).sums[0];
+    }
+    info.true_residual = std::sqrt(rr / bb);
+    const bool relative_ok = prm.abs_tol || info.true_residual <= prm.tol;
+    if (S.status != ST_CONVERGED || relative_ok || restart >= 4 || total_iter >= prm.maxiter) {
+      if (S.status == ST_CONVERGED && !relative_ok) info.status = ST_MAXITER;
+      break;
+    }
+    // the preconditioned residual met tol2 but the full one did not: tighten and resume from x64
+    tol2 *= 0.25 * (prm.tol * prm.tol * bb) / std::max(rr, 1e-300);
+    info.restarts++;
+  }
+  info.iterations = total_iter;
+  info.updates = total_updates;
+  launch_convert(SOA64, AOS64, Vh, w.xe.data.p, nullptr, xp, nullptr, st);
+  launch_convert(SOA64, AOS64, Vh, w.x64.data.p, nullptr, xp + half, nullptr, st);
+  QCU_CUDA(cudaStreamSynchronize(st));
+  info.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return info;
+}
+
+// ---------------------------------------------------------------- operators on a handle
+void handle_dslash(GaugeHandle &G, void *out, const void *in, int par, int use_clover, int precision) {
+  require(out && in, "dslash: null spinor pointer");
+  require(par == 0 || par == 1, "parity must be 0 or 1");
+  require(!use_clover || G.has_clover, "dslash: no clover term loaded");
+  const int kind = kind_of_precision(precision);
+  Context &ctx = context();
+  std::lock_guard<std::mutex> lk(ctx.mu);
+  Workspace &w = workspace();
+  const int Vh = G.g.Vh;
+  w.aux.alloc(SOA64, Vh);
+  w.tmp64.alloc(SOA64, Vh);
+  w.r.alloc(kind, Vh);
+  w.tmp.alloc(kind, Vh);
+  Spinor &a = kind == SOA64 ? w.aux : w.r, &b = kind == SOA64 ? w.tmp64 : w.tmp;
+  QCU_CUDA(cudaDeviceSynchronize());
+  Dsl d{G, ctx, kind};
+  launch_convert(AOS64, kind, Vh, in, nullptr, a.data.p, a.norm.as<float>(), ctx.stream);
+  d(par, a, b, use_clover != 0, 1.0);
+  launch_convert(kind, AOS64, Vh, b.data.p, b.norm.as<float>(), out, nullptr, ctx.stream);
+  QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+void handle_mpc(GaugeHandle &G, void *out, const void *in, double kappa, int use_clover) {
+  require(out && in, "mpc: null spinor pointer");
+  require(!use_clover || G.has_clover, "mpc: no clover term loaded");
+  Context &ctx = context();
+  std::lock_guard<std::mutex> lk(ctx.mu);
+  Workspace &w = workspace();
+  const int Vh = G.g.Vh;
+  w.aux.alloc(SOA64, Vh);
+  w.tmp64.alloc(SOA64, Vh);
+  w.r64.alloc(SOA64, Vh);
+  QCU_CUDA(cudaDeviceSynchronize());
+  Dsl d64{G, ctx, SOA64};
+  launch_convert(AOS64, SOA64, Vh, in, nullptr, w.aux.data.p, nullptr, ctx.stream);
+  d64(0, w.aux, w.tmp64, use_clover != 0, 1.0);
+  d64(1, w.tmp64, w.r64, use_clover != 0, -kappa * kappa, &w.aux, 1.0);
+  launch_convert(SOA64, AOS64, Vh, w.r64.data.p, nullptr, out, nullptr, ctx.stream);
+  QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+void handle_mat(GaugeHandle &G, void *out, const void *in, double kappa, int use_clover) {
+  require(out && in, "mat: null spinor pointer");
+  require(!use_clover || G.has_clover, "mat: no clover term loaded");
+  Context &ctx = context();
+  std::lock_guard<std::mutex> lk(ctx.mu);
+  Workspace &w = workspace();
+  const int Vh = G.g.Vh;
+  for (Spinor *q : {&w.be, &w.bo, &w.tmp64, &w.aux}) q->alloc(SOA64, Vh);
+  QCU_CUDA(cudaDeviceSynchronize());
+  Dsl d64{G, ctx, SOA64};
+  const size_t half = spinor_bytes(AOS64, Vh);
+  launch_convert(AOS64, SOA64, Vh, in, nullptr, w.be.data.p, nullptr, ctx.stream);
+  launch_convert(AOS64, SOA64, Vh, static_cast<const char *>(in) + half, nullptr, w.bo.data.p, nullptr, ctx.stream);
+  for (int p = 0; p < 2; p++) {
+    Spinor &xp = p ? w.bo : w.be;
+    const Spinor *ax = &xp;
+    if (use_clover) {
+      launch_clover_apply(SOA64, Vh, G.A64[p].p, xp.data.p, w.aux.data.p, ctx.stream);
+      ax = &w.aux;
+    }
+    d64(p, p ? w.be : w.bo, w.tmp64, false, -kappa, ax, 1.0);
+    launch_convert(SOA64, AOS64, Vh, w.tmp64.data.p, nullptr, static_cast<char *>(out) + p * half, nullptr,
+                   ctx.stream);
+  }
+  QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+// ---------------------------------------------------------------- legacy direct path
+void legacy_dslash(void *out, const void *in, const void *gauge, const int latt[4], int parity, int clover) {
+  require(out && in && gauge, "dslash: null pointer argument");
+  require(parity == 0 || parity == 1, "parity must be 0 or 1");
+  const Geom g = make_geom(latt);
+  Context &ctx = context();
+  std::lock_guard<std::mutex> lk(ctx.mu);
+  QCU_CUDA(cudaDeviceSynchronize());
+  DslashArgs d;
+  d.in = in;
+  d.out = out;
+  d.gauge = gauge;
+  d.parity = parity;
+  d.t_bc = 1.0;
+  d.a = 1.0;
+  static DevBuf *cl = new DevBuf(), *bad = new DevBuf();  // reused across calls, never freed
+  if (clover) {
+    // qcu builds the clover of the output parity with unit normalisation on
+    // every call (src/nccl_clover_dslash.cu:27-61)
+    cl->ensure(clover_bytes(CSOA64, g.Vh));
+    bad->ensure(sizeof(int));
+    QCU_CUDA(cudaMemsetAsync(bad->p, 0, sizeof(int), ctx.stream));
+    launch_clover_build(g, gauge, parity, 1.0, nullptr, cl->p, bad->as<int>(), ctx.stream);
+    d.clover = cl->p;
+  }
+  launch_dslash(AOS64, GAOS64, CSOA64, g, d, ctx, ctx.stream);
+  QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+  if (clover) {
+    int nbad = 0;
+    QCU_CUDA(cudaMemcpy(&nbad, bad->p, sizeof(int), cudaMemcpyDeviceToHost));
+    require(nbad == 0, "clover term is singular on " + std::to_string(nbad) + " site blocks");
+  }
+}
+
+}  // namespace qcu

@@ -1,0 +1,205 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle on the
+same seeded inputs.  Tolerances: FP64 <= 1e-13 relative (legacy dslash),
+FP32 <= 1e-6, FP16 storage <= 2e-3; solves to a 1e-10 FP64 true residual."""
+import numpy as np
+import pytest
+
+import oracle as O
+from util import dev, empty_like_dev, host, rel
+
+pytestmark = pytest.mark.gpu
+
+LATTS = [[4, 4, 4, 4], [8, 8, 8, 8], [6, 4, 2, 10], [2, 2, 2, 2], [4, 6, 8, 12]]
+
+
+@pytest.fixture(scope="module")
+def q():
+    import qcu_b200
+
+    return qcu_b200
+
+
+def _fields(latt, kind="haar", seed=1):
+    U = O.gauge_haar(latt, seed) if kind == "haar" else O.gauge_smooth(latt, 0.3, seed)
+    psi = O.fermion_gauss(O.full_shape(latt), seed + 100)
+    return U, psi
+
+
+@pytest.mark.parametrize("latt", LATTS)
+@pytest.mark.parametrize("kind", ["haar", "smooth"])
+def test_dslashQcu_fp64(q, latt, kind):
+    U, psi = _fields(latt, kind)
+    dU, dpsi = dev(U), dev(psi)
+    for p in (0, 1):
+        out = empty_like_dev(O.half_shape(latt))
+        q.dslashQcu(out, dpsi[1 - p], dU, q.QcuParam(latt), p)
+        assert q.last_error()[0] == 0
+        assert rel(host(out), O.dslash(psi[1 - p], U, latt, p)) <= 1e-13
+    # inputs untouched (qcu permuted them in place and restored them)
+    assert np.array_equal(host(dU), U) and np.array_equal(host(dpsi), psi)
+
+
+def test_ncclDslashQcu_and_grid_check(q):
+    latt = [8, 4, 4, 8]
+    U, psi = _fields(latt)
+    dU, dpsi = dev(U), dev(psi)
+    out = empty_like_dev(O.half_shape(latt))
+    q.ncclDslashQcu(out, dpsi[0], dU, q.QcuParam(latt), 1, q.QcuParam([1, 1, 1, 1]))
+    assert rel(host(out), O.dslash(psi[0], U, latt, 1)) <= 1e-13
+    out2 = empty_like_dev(O.half_shape(latt))
+    q.ncclDslashQcu(out2, dpsi[0], dU, q.QcuParam(latt), 1, q.QcuParam([2, 1, 1, 1]))
+    code, msg = q.last_error()
+    assert code != 0 and "grid" in msg
+    assert np.isnan(host(out2)).all()  # nothing written
+    q.mpiDslashQcu(out2, dpsi[0], dU, q.QcuParam(latt), 1, q.QcuParam([1, 1, 1, 1]))  # no-op, as in qcu
+    assert np.isnan(host(out2)).all()
+
+
+def test_bad_arguments_do_not_crash(q):
+    latt = [5, 4, 4, 4]  # odd Lx
+    out = empty_like_dev((10,))
+    q.dslashQcu(out, out, out, q.QcuParam(latt), 0)
+    assert q.last_error()[0] == 1
+    q.dslashQcu(out, out, out, q.QcuParam([4, 4, 4, 4]), 2)
+    assert q.last_error()[0] == 1
+    q.dslashQcu(None, out, out, q.QcuParam([4, 4, 4, 4]), 0)
+    assert q.last_error()[0] == 1
+
+
+@pytest.mark.parametrize("latt,kind", [([4, 4, 4, 4], "smooth"), ([4, 4, 2, 8], "smooth"), ([4, 4, 4, 4], "haar")])
+def test_dslashCloverQcu(q, latt, kind):
+    U, psi = _fields(latt, kind, seed=3)
+    dU, dpsi = dev(U), dev(psi)
+    for p in (0, 1):
+        A = O.clover_build(U, latt, p, 1.0)
+        cond = np.linalg.cond(A).max()
+        expect = O.clover_apply(O.clover_invert(A), O.dslash(psi[1 - p], U, latt, p))
+        out = empty_like_dev(O.half_shape(latt))
+        q.dslashCloverQcu(out, dpsi[1 - p], dU, q.QcuParam(latt), p)
+        assert q.last_error()[0] == 0
+        assert rel(host(out), expect) <= 1e-14 * max(cond, 10)
+
+
+@pytest.mark.parametrize("t_bc", [1.0, -1.0])
+@pytest.mark.parametrize("prec,tol", [(64, 1e-13), (32, 1e-6), (16, 2e-3)])
+def test_ext_dslash_precisions(q, t_bc, prec, tol):
+    latt = [8, 4, 6, 8]
+    U, psi = _fields(latt, "smooth", 5)
+    with q.Gauge(dev(U), latt, t_boundary=t_bc) as G:
+        for p in (0, 1):
+            out = empty_like_dev(O.half_shape(latt))
+            G.dslash(out, dev(psi[1 - p]), p, precision=prec)
+            assert rel(host(out), O.dslash(psi[1 - p], U, latt, p, t_bc)) <= tol
+
+
+@pytest.mark.parametrize("prec,tol", [(64, 1e-13), (32, 1e-6)])
+def test_ext_clover_dslash_csw(q, prec, tol):
+    latt = [4, 4, 6, 8]
+    U, psi = _fields(latt, "smooth", 6)
+    kappa, csw = 0.12, 1.0
+    with q.Gauge(dev(U), latt, t_boundary=-1.0, clover_coeff=kappa * csw) as G:
+        for p in (0, 1):
+            Ainv = O.clover_invert(O.clover_build(U, latt, p, kappa * csw))
+            expect = O.clover_apply(Ainv, O.dslash(psi[1 - p], U, latt, p, -1.0))
+            out = empty_like_dev(O.half_shape(latt))
+            G.dslash(out, dev(psi[1 - p]), p, clover=True, precision=prec)
+            assert rel(host(out), expect) <= tol
+
+
+@pytest.mark.parametrize("clover", [False, True])
+def test_ext_matpc_and_mat(q, clover):
+    latt = [4, 6, 4, 8]
+    U, psi = _fields(latt, "smooth", 7)
+    kappa = 0.11
+    c = kappa * 1.0
+    with q.Gauge(dev(U), latt, t_boundary=-1.0, clover_coeff=c if clover else 0.0) as G:
+        A = [O.clover_build(U, latt, p, c) for p in (0, 1)] if clover else [None, None]
+        Ai = [O.clover_invert(a) for a in A] if clover else [None, None]
+        out = empty_like_dev(O.half_shape(latt))
+        G.matpc(out, dev(psi[1]), kappa, clover=clover)
+        assert rel(host(out), O.mpc(psi[1], U, latt, kappa, 1, -1.0, True, Ai[1], Ai[0])) <= 1e-13
+        full = empty_like_dev(O.full_shape(latt))
+        G.mat(full, dev(psi), kappa, clover=clover)
+        assert rel(host(full), O.mfull(psi, U, latt, kappa, -1.0, True, A[0], A[1])) <= 1e-13
+
+
+def test_generators_match_oracle(q):
+    import torch
+
+    latt = [4, 4, 6, 8]
+    for kind, ref in ((0, O.gauge_haar(latt, 77)), (1, O.gauge_smooth(latt, 0.25, 77))):
+        g = torch.empty(O.gauge_shape(latt), dtype=torch.complex128, device="cuda")
+        q.gauge_random(g, latt, kind, 0.25, 77)
+        assert rel(host(g), ref) < 1e-13
+    f = torch.empty(O.full_shape(latt), dtype=torch.complex128, device="cuda")
+    q.fermion_random(f, f.numel(), 0, 5)
+    assert rel(host(f), O.fermion_gauss(O.full_shape(latt), 5)) < 1e-14
+    q.fermion_random(f, f.numel(), 1, 5)
+    assert np.array_equal(host(f), O.fermion_uniform(O.full_shape(latt), 5))
+
+
+def test_ncclBistabCgQcu(q):
+    """qcu's solver semantics: kappa = 0.125, random start, ||r_o||^2 < 1e-9."""
+    latt = [8, 8, 8, 8]
+    U = O.gauge_haar(latt, 2)
+    b = np.ones(O.full_shape(latt), complex)  # the reference test's source (test.nccl.bistabcg.qcu-np1.py:30)
+    x = empty_like_dev(O.full_shape(latt))
+    q.ncclBistabCgQcu(x, dev(b), dev(U), q.QcuParam(latt), q.QcuParam([1, 1, 1, 1]))
+    assert q.last_error()[0] == 0
+    xg = host(x)
+    x0 = np.zeros_like(b)
+    x0[1] = O.fermion_uniform(O.half_shape(latt), 23333)
+    xo, it, res2 = O.solve_full(b, U, latt, 0.125, x0=x0, tol=1e-9, abs_tol=True, maxiter=1000)
+    r = b - O.mfull(xg, U, latt, 0.125)
+    assert np.linalg.norm(r) ** 2 < 1e-9
+    assert rel(xg, xo) < 1e-6
+
+
+@pytest.mark.parametrize("prec", [64, 32, 16])
+@pytest.mark.parametrize("clover", [False, True])
+def test_invert_true_residual(q, prec, clover):
+    latt = [8, 8, 8, 16]
+    U = O.gauge_smooth(latt, 0.25, 9)
+    b = O.fermion_gauss(O.full_shape(latt), 19)
+    kappa = 0.125
+    c = kappa * 1.0
+    A = [O.clover_build(U, latt, p, c) for p in (0, 1)] if clover else [None, None]
+    with q.Gauge(dev(U), latt, t_boundary=-1.0, clover_coeff=c if clover else 0.0) as G:
+        x = empty_like_dev(O.full_shape(latt))
+        info = G.invert(x, dev(b), kappa, tol=1e-10, maxiter=5000, precision=prec, delta=0.1, clover=clover)
+    assert info["status"] == 1, info
+    assert info["true_residual"] <= 1e-10
+    xg = host(x)
+    r = b - O.mfull(xg, U, latt, kappa, -1.0, True, A[0], A[1])
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05e-10
+    # same solution as the FP64 oracle solve (error bounded by the condition number)
+    kw = dict(Ainv_e=O.clover_invert(A[0]), Ainv_o=O.clover_invert(A[1])) if clover else {}
+    xo, it, _ = O.solve_full(b, U, latt, kappa, t_bc=-1.0, tol=1e-12, maxiter=5000, **kw)
+    assert rel(xg, xo) < 1e-7
+    if prec == 64:
+        assert abs(info["iterations"] - it) <= max(3, 0.1 * it)
+
+
+def test_invert_zero_source_and_initial_guess(q):
+    latt = [4, 4, 4, 8]
+    U = O.gauge_smooth(latt, 0.25, 3)
+    with q.Gauge(dev(U), latt) as G:
+        x = empty_like_dev(O.full_shape(latt))
+        info = G.invert(x, dev(np.zeros(O.full_shape(latt), complex)), 0.12)
+        assert info["status"] == 1 and np.abs(host(x)).max() == 0
+        b = O.fermion_gauss(O.full_shape(latt), 1)
+        x = dev(np.zeros(O.full_shape(latt), complex))
+        i1 = G.invert(x, dev(b), 0.12, tol=1e-10)
+        i2 = G.invert(x, dev(b), 0.12, tol=1e-10, x0_mode=1)  # restart from the solution
+        assert i2["iterations"] <= 2 and i2["true_residual"] <= 1e-10 and i1["iterations"] > 10
+
+
+def test_invert_maxiter_reports_status(q):
+    latt = [4, 4, 4, 8]
+    U = O.gauge_smooth(latt, 0.25, 3)
+    b = O.fermion_gauss(O.full_shape(latt), 2)
+    with q.Gauge(dev(U), latt) as G:
+        x = empty_like_dev(O.full_shape(latt))
+        info = G.invert(x, dev(b), 0.124, tol=1e-12, maxiter=3)
+    assert info["status"] == 2 and info["iterations"] == 3
+    assert np.isfinite(host(x)).all()
