@@ -311,7 +311,7 @@ def run_ours(args, world, rank, local, pg):
             "metric": METRIC, "value": round(per_solve, 4), "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(per_solve * 1e3, 2), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": {64: "f64", 32: "f32 storage / f64 reductions", 16: "f16+norm storage / f32 math / f64 reductions"}[
+            "dtype": {64: "f64", 32: "f32 storage / f64 reductions", 16: "int16+norm storage / f32 math / f64 reductions"}[
                 args.precision],
             "data": "synthetic (seeded smooth SU(3) gauge, Gaussian source)",
             "config": {"workload": "wilson-bicgstab-32^3x64-smooth-eps0.25", "latt": latt, "kappa": args.kappa,

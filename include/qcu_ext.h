@@ -27,7 +27,7 @@ int qcuGetLastError(char *msg, int len);
 int qcuVersion(void);
 
 /* Load a gauge field (PyQuda layout) onto the device as reconstruct-12
- * storage in FP64, FP32 and FP16.  t_boundary = +1 periodic, -1 antiperiodic
+ * storage in FP64, FP32 and 16-bit fixed point.  t_boundary = +1 periodic, -1 antiperiodic
  * in time (applied in the stencil, so the links stay SU(3)).  clover_coeff
  * != 0 also builds the clover term A = 1 - coeff/8 sum_{mu<nu} gamma_mu
  * gamma_nu (Q_munu - Q_munu^dag) and its inverse on both parities; coeff =
@@ -37,7 +37,7 @@ int qcuGaugeLoad(qcuGauge *h, const void *gauge, const int latt[4], double t_bou
 int qcuGaugeFree(qcuGauge h);
 
 /* half spinors: out(parity) = [A_parity^{-1}] D_{parity <- 1-parity} in, computed
- * with the field stored in `precision` bits (64, 32, or 16 = FP16 + per-site
+ * with the field stored in `precision` bits (64, 32, or 16 = int16 fixed point + per-site
  * norm; accumulation in FP64 resp. FP32); input and output stay complex128 */
 int qcuDslash(qcuGauge h, void *out, const void *in, int parity, int use_clover, int precision);
 /* odd-parity Schur operator M_pc = 1 - kappa^2 [A_o^-1] D_oe [A_e^-1] D_eo */
@@ -49,7 +49,7 @@ typedef struct {
   double kappa;
   double tol;            /* stop when ||b - M x|| <= tol ||b|| (FP64, full system) */
   int maxiter;
-  int precision;         /* inner precision: 64, 32 or 16 (FP16 + per-site norm) */
+  int precision;         /* inner precision: 64, 32 or 16 (int16 + per-site norm) */
   double delta;          /* reliable update threshold (0.1 typical; 0 = only at the end) */
   int abs_tol;           /* 1: qcu's test, iterated ||r_o||^2 < tol */
   int x0_mode;           /* 0 zero, 1 use x on input, 2 uniform (0,1] from x0_seed */

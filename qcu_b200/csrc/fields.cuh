@@ -7,14 +7,16 @@
 //   SOA64 : double2 [12][stride]    component-major, one 16-byte load per
 //           component, 512 contiguous bytes per warp instruction.
 //   SOA32 : float4  [6][stride]     two complex components per 16-byte load.
-//   SOA16 : uint4   [3][stride] + float norm[stride]   FP16 values scaled by
-//           the per-site max |component| (four complex per 16-byte load).
+//   SOA16 : uint4   [3][stride] + float norm[stride]   16-bit fixed point
+//           (int16, value/norm * 32767) scaled by the per-site max |component|,
+//           four complex per 16-byte load.  Fixed point keeps 15 bits of
+//           mantissa relative to the site maximum where FP16 keeps 11.
 // Gauge kinds (reconstruct-12: rows 0 and 1 stored, row 2 = conj(r0 x r1),
 // include/define.h:198-206):
 //   GAOS64 : PyQuda layout complex128 [dir][par][site][3][3], rows 0-1 read
 //   GSOA64 : double2 [dir][par][6][stride]
 //   GSOA32 : float4  [dir][par][3][stride]
-//   GSOA16 : uint2   [dir][par][3][stride]   (four FP16 per load, |U_ij| <= 1)
+//   GSOA16 : uint2   [dir][par][3][stride]   (four int16 fixed point per load, |U_ij| <= 1)
 #pragma once
 #include "cplx.cuh"
 
@@ -26,6 +28,23 @@ enum GaugeKind { GAOS64 = 0, GSOA64 = 1, GSOA32 = 2, GSOA16 = 3 };
 template <int K> struct SpinorReal { using T = float; };
 template <> struct SpinorReal<AOS64> { using T = double; };
 template <> struct SpinorReal<SOA64> { using T = double; };
+
+// 16-bit fixed point: two signed 16-bit values per 32-bit word
+constexpr float FIX16_SCALE = 32767.0f;
+__device__ __forceinline__ unsigned fix16_pack(float a, float b) {
+  const int ia = __float2int_rn(a * FIX16_SCALE), ib = __float2int_rn(b * FIX16_SCALE);
+  return ((unsigned)ia & 0xffffu) | ((unsigned)ib << 16);
+}
+// decode without int->float conversions: flipping the sign bits turns each
+// signed half into an offset-binary u = v + 32768; byte-permuting u under the
+// exponent bits of 2^23 gives the float 2^23 + u exactly, and subtracting
+// 2^23 + 32768 (exact, same exponent) leaves v.
+__device__ __forceinline__ float2 fix16_unpack(unsigned w) {
+  const unsigned x = w ^ 0x80008000u;
+  const float lo = __int_as_float(__byte_perm(x, 0x4B000000u, 0x7610)) - 8421376.0f;
+  const float hi = __int_as_float(__byte_perm(x, 0x4B000000u, 0x7632)) - 8421376.0f;
+  return make_float2(lo, hi);
+}
 
 // Lattice geometry of one parity (half lattice).  Site index
 // i = ((t*Lz + z)*Ly + y)*Lxh + xh, the PyQuda/qcu ordering.
@@ -69,15 +88,14 @@ __device__ __forceinline__ void spinor_load(const SpinorView<K> &v, int s, Cpx<T
     }
   } else {
     const uint4 *p = static_cast<const uint4 *>(v.p) + s;
-    float nrm = __ldg(v.norm + s);
+    const float nrm = __ldg(v.norm + s) * (1.0f / FIX16_SCALE);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       uint4 d = __ldg(p + (size_t)c * v.stride);
       unsigned w[4] = {d.x, d.y, d.z, d.w};
 #pragma unroll
       for (int k = 0; k < 4; k++) {
-        __half2 h = *reinterpret_cast<__half2 *>(&w[k]);
-        float2 f = __half22float2(h);
+        const float2 f = fix16_unpack(w[k]);
         out[4 * c + k] = Cpx<T>((T)(f.x * nrm), (T)(f.y * nrm));
       }
     }
@@ -110,10 +128,7 @@ __device__ __forceinline__ void spinor_store(const SpinorView<K> &v, int s, cons
     for (int c = 0; c < 3; c++) {
       unsigned w[4];
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        __half2 h = __floats2half2_rn((float)in[4 * c + k].re * inv, (float)in[4 * c + k].im * inv);
-        w[k] = *reinterpret_cast<unsigned *>(&h);
-      }
+      for (int k = 0; k < 4; k++) w[k] = fix16_pack((float)in[4 * c + k].re * inv, (float)in[4 * c + k].im * inv);
       p[(size_t)c * v.stride] = make_uint4(w[0], w[1], w[2], w[3]);
     }
     v.norm[s] = mx;
@@ -161,8 +176,8 @@ __device__ __forceinline__ void link_load(const GaugeView<G> &u, int dir, int pa
       unsigned w[2] = {d.x, d.y};
 #pragma unroll
       for (int q = 0; q < 2; q++) {
-        float2 f = __half22float2(*reinterpret_cast<__half2 *>(&w[q]));
-        m[2 * k + q] = Cpx<T>((T)f.x, (T)f.y);
+        const float2 f = fix16_unpack(w[q]);
+        m[2 * k + q] = Cpx<T>((T)(f.x * (1.0f / FIX16_SCALE)), (T)(f.y * (1.0f / FIX16_SCALE)));
       }
     }
   }

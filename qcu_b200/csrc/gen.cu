@@ -179,11 +179,9 @@ __global__ void k_gauge_pack(int Vh, const double2 *__restrict__ in, void *out) 
     } else {
       uint2 *o = static_cast<uint2 *>(out) + slab * 3 * Vh + s;
 #pragma unroll
-      for (int k = 0; k < 3; k++) {
-        __half2 a = __floats2half2_rn((float)v[2 * k].x, (float)v[2 * k].y);
-        __half2 b = __floats2half2_rn((float)v[2 * k + 1].x, (float)v[2 * k + 1].y);
-        o[(size_t)k * Vh] = make_uint2(*reinterpret_cast<unsigned *>(&a), *reinterpret_cast<unsigned *>(&b));
-      }
+      for (int k = 0; k < 3; k++)
+        o[(size_t)k * Vh] = make_uint2(fix16_pack((float)v[2 * k].x, (float)v[2 * k].y),
+                                       fix16_pack((float)v[2 * k + 1].x, (float)v[2 * k + 1].y));
     }
   }
 }

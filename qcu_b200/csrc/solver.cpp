@@ -276,12 +276,19 @@ SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParam
       }
       if (exec) cudaGraphExecDestroy(exec);
     }
-    // fold whatever the inner solution still holds
-    launch_xfold(w.x.kind, Vh, vs, ctx.st, GATE_ALWAYS, st);
+    // fold whatever the inner solution still holds (after a NaN the inner
+    // partial solution is discarded: x64 is the last good FP64 iterate)
+    if (S.status != ST_NAN) launch_xfold(w.x.kind, Vh, vs, ctx.st, GATE_ALWAYS, st);
     total_iter += S.iter;
     total_updates += S.nupdates;
     info.status = S.status;
     info.iter_residual2 = S.rr;
+    // BiCGSTAB breakdown (rho, <rt,v> or <t,t> vanishing) or a non-finite
+    // inner value: restart from the FP64 iterate with a fresh shadow residual
+    if ((S.status == ST_BREAKDOWN || S.status == ST_NAN) && info.restarts < 8 && total_iter < prm.maxiter) {
+      info.restarts++;
+      continue;
+    }
     // x_e = A_e^-1 (b_e + kappa D_eo x_o)
     d64(0, w.x64, w.tmp64, false, kappa, &w.be, 1.0);
     if (clov) launch_clover_apply(SOA64, Vh, G.Ainv64[0].p, w.tmp64.data.p, w.xe.data.p, st);
@@ -301,7 +308,7 @@ SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParam
     }
     info.true_residual = std::sqrt(rr / bb);
     const bool relative_ok = prm.abs_tol || info.true_residual <= prm.tol;
-    if (S.status != ST_CONVERGED || relative_ok || restart >= 4 || total_iter >= prm.maxiter) {
+    if (S.status != ST_CONVERGED || relative_ok || restart >= 12 || total_iter >= prm.maxiter) {
       if (S.status == ST_CONVERGED && !relative_ok) info.status = ST_MAXITER;
       break;
     }

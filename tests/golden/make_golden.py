@@ -85,7 +85,8 @@ def main(outdir):
     U = O.gauge_haar(latt, 6)
     b = np.ones(O.full_shape(latt), complex)
     dx = torch.zeros(O.full_shape(latt), dtype=torch.complex128, device="cuda")
-    lib.ncclBistabCgQcu(dx.data_ptr(), d(b).data_ptr(), d(U).data_ptr(), ctypes.byref(param(latt)),
+    db, dU = d(b), d(U)  # keep the tensors alive across the call
+    lib.ncclBistabCgQcu(dx.data_ptr(), db.data_ptr(), dU.data_ptr(), ctypes.byref(param(latt)),
                         ctypes.byref(grid))
     torch.cuda.synchronize()
     out["s_latt"] = np.array(latt)

@@ -27,6 +27,23 @@ def test_oracle_dslash_matches_qcu(g, tag, api):
         assert rel(O.dslash(psi[1 - p], U, latt, p), g[f"{tag}_{api}_p{p}"]) <= 1e-14
 
 
+def _gj_growth(A):
+    """max |A| / min |pivot| of the unpivoted Gauss-Jordan qcu runs per site
+    (include/define.h:334-365): the factor by which it amplifies rounding."""
+    worst = 1.0
+    for M in A:
+        M = M.copy()
+        piv = []
+        for i in range(12):
+            piv.append(abs(M[i, i]))
+            M[i] /= M[i, i]
+            for j in range(12):
+                if j != i:
+                    M[j] -= M[j, i] * M[i]
+        worst = max(worst, np.abs(A).max() / min(piv))
+    return worst
+
+
 @pytest.mark.parametrize("tag", ["c4s", "c4h"])
 def test_oracle_clover_matches_qcu(g, tag):
     latt = list(g[f"{tag}_latt"])
@@ -34,8 +51,14 @@ def test_oracle_clover_matches_qcu(g, tag):
     for p in (0, 1):
         A = O.clover_build(U, latt, p, 1.0)
         expect = O.clover_apply(O.clover_invert(A), O.dslash(psi[1 - p], U, latt, p))
-        cond = np.linalg.cond(A).max()
-        assert rel(expect, g[f"{tag}_dslashCloverQcu_p{p}"]) <= 1e-14 * max(cond, 10)
+        got = g[f"{tag}_dslashCloverQcu_p{p}"]
+        # both sides run an unpivoted elimination; on hot links some sites have
+        # tiny intermediate pivots, so the bound scales with the growth squared
+        tol = 1e-15 * max(_gj_growth(A), 10.0) ** 2
+        assert rel(expect, got) <= tol
+        # and where the elimination is benign the agreement is at rounding level
+        if tag == "c4s":
+            assert rel(expect, got) <= 1e-11
 
 
 def test_qcu_solver_output_solves_the_oracle_system(g):
@@ -46,4 +69,4 @@ def test_qcu_solver_output_solves_the_oracle_system(g):
     # previous iterate (include/lattice_bistabcg.h:301-332)
     assert np.linalg.norm(r) ** 2 < 1e-7
     xo, it, _ = O.solve_full(b, U, latt, 0.125, tol=1e-12, maxiter=1000)
-    assert rel(x, xo) < 1e-4
+    assert rel(x, xo) < 1e-5

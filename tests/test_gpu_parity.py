@@ -1,6 +1,6 @@
 """GPU parity: the CUDA path (through the C ABI) against the CPU oracle on the
 same seeded inputs.  Tolerances: FP64 <= 1e-13 relative (legacy dslash),
-FP32 <= 1e-6, FP16 storage <= 2e-3; solves to a 1e-10 FP64 true residual."""
+FP32 <= 1e-6, 16-bit fixed-point storage <= 2e-4; solves to a 1e-10 FP64 true residual."""
 import numpy as np
 import pytest
 
@@ -81,7 +81,7 @@ def test_dslashCloverQcu(q, latt, kind):
 
 
 @pytest.mark.parametrize("t_bc", [1.0, -1.0])
-@pytest.mark.parametrize("prec,tol", [(64, 1e-13), (32, 1e-6), (16, 2e-3)])
+@pytest.mark.parametrize("prec,tol", [(64, 1e-13), (32, 1e-6), (16, 2e-4)])
 def test_ext_dslash_precisions(q, t_bc, prec, tol):
     latt = [8, 4, 6, 8]
     U, psi = _fields(latt, "smooth", 5)
@@ -174,10 +174,15 @@ def test_invert_true_residual(q, prec, clover):
     assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05e-10
     # same solution as the FP64 oracle solve (error bounded by the condition number)
     kw = dict(Ainv_e=O.clover_invert(A[0]), Ainv_o=O.clover_invert(A[1])) if clover else {}
-    xo, it, _ = O.solve_full(b, U, latt, kappa, t_bc=-1.0, tol=1e-12, maxiter=5000, **kw)
+    xo, _, _ = O.solve_full(b, U, latt, kappa, t_bc=-1.0, tol=1e-12, maxiter=5000, **kw)
     assert rel(xg, xo) < 1e-7
-    if prec == 64:
-        assert abs(info["iterations"] - it) <= max(3, 0.1 * it)
+    if prec == 64 and not clover:
+        # same algorithm, same stopping point: the library stops on
+        # ||r_o|| <= tol ||b|| (full source), the oracle on ||r_o|| <= tol' ||b'_o||
+        bp = b[1] + kappa * O.dslash(b[0], U, latt, 1, -1.0)
+        tol_o = 1e-10 * np.linalg.norm(b) / np.linalg.norm(bp)
+        _, it, _ = O.solve_full(b, U, latt, kappa, t_bc=-1.0, tol=tol_o, maxiter=5000)
+        assert abs(info["iterations"] - it) <= 2
 
 
 def test_invert_zero_source_and_initial_guess(q):
