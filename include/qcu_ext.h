@@ -16,6 +16,8 @@
 #ifndef QCU_B200_QCU_EXT_H
 #define QCU_B200_QCU_EXT_H
 
+#include "qcu.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -77,6 +79,22 @@ int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuIn
  * fermion kind: 0 complex normal N(0,1) per component, 1 uniform (0,1]. */
 int qcuGaugeRandom(void *gauge, const int latt[4], int kind, double eps, unsigned long long seed);
 int qcuFermionRandom(void *psi, long long n_complex, int kind, unsigned long long seed);
+
+/* dslashCloverQcu for callers that cannot allocate device memory.  This entry
+ * point has no counterpart in the reference.  Callers such as a framework
+ * whose caching allocator already holds its device-memory budget, a job under
+ * a hard device-memory cap, or a latency-critical path cannot afford a
+ * cudaMalloc; this variant keeps the inverse clover field it needs in a
+ * static device array (18 MiB, held by every GPU that loads the library) and
+ * allocates nothing.  Same arguments and result as dslashCloverQcu; returns 0
+ * on success, non-zero with qcuGetLastError() set otherwise.
+ *  - at most qcuNoAllocMaxSites() = 32768 sites per parity (a 16^4 lattice);
+ *    larger lattices are rejected with an error;
+ *  - the first call on a device sets up the scratch address with that device
+ *    current; make it before any stream capture;
+ *  - all calls share the scratch: calls that overlap on the GPU race. */
+int dslashCloverQcuNoAlloc(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, int parity);
+int qcuNoAllocMaxSites(void);
 
 /* number of kernels this library has launched in this process (graph
  * replays count every node) */

@@ -113,6 +113,9 @@ _lib.qcuInvert.argtypes = [_vp, _vp, _vp, ctypes.POINTER(QcuInvertParam), ctypes
 _lib.qcuGaugeRandom.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong]
 _lib.qcuFermionRandom.argtypes = [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_ulonglong]
 _lib.qcuGetStream.restype = _vp
+_lib.dslashCloverQcuNoAlloc.argtypes = [_vp, _vp, _vp, _P, ctypes.c_int]
+_lib.dslashCloverQcuNoAlloc.restype = ctypes.c_int
+_lib.qcuNoAllocMaxSites.restype = ctypes.c_int
 _lib.qcuKernelLaunches.restype = ctypes.c_longlong
 _lib.qcuBenchDslash.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
 
@@ -182,6 +185,18 @@ def ncclBistabCgQcu(fermion_out, fermion_in, gauge, param, grid) -> None:
 
 
 # ------------------------------------------------------------------ qcu_ext.h
+def dslashCloverQcuNoAlloc(fermion_out, fermion_in, gauge, param, parity: int) -> int:
+    """dslashCloverQcu without device allocation: the inverse clover scratch
+    lives in a static device array, so lattices are limited to
+    ``noalloc_max_sites()`` sites per parity; returns the status code."""
+    return int(_lib.dslashCloverQcuNoAlloc(_ptr(fermion_out), _ptr(fermion_in), _ptr(gauge),
+                                           ctypes.byref(_param(param)), int(parity)))
+
+
+def noalloc_max_sites() -> int:
+    return int(_lib.qcuNoAllocMaxSites())
+
+
 def _latt(latt):
     return (ctypes.c_int * 4)(*[int(v) for v in latt])
 

@@ -12,6 +12,8 @@
 
 namespace qcu {
 int last_error(char *buf, int len);
+void clover_dslash_noalloc(void *out, const void *in, const void *gauge, const int latt[4], int parity);
+int noalloc_max_vh();
 }
 
 using namespace qcu;
@@ -212,6 +214,15 @@ int qcuFermionRandom(void *psi, long long n, int kind, unsigned long long seed) 
   QCU_CUDA(cudaStreamSynchronize(ctx.stream));
   QCU_API_END
 }
+
+int dslashCloverQcuNoAlloc(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, int parity) {
+  QCU_API_BEGIN
+  require(param != nullptr, "param pointer is null");
+  clover_dslash_noalloc(fermion_out, fermion_in, gauge, param->lattice_size, parity);
+  QCU_API_END
+}
+
+int qcuNoAllocMaxSites(void) { return noalloc_max_vh(); }
 
 long long qcuKernelLaunches(void) { return launch_count(); }
 
