@@ -58,11 +58,16 @@ typedef struct {
   unsigned long long x0_seed;
   int use_clover;
   int chunk;             /* iterations per captured CUDA graph (0 = automatic) */
+  int solver;            /* 0 BiCGSTAB with reliable updates; 1 flexible GCR (FP64) whose
+                            preconditioner is an inner BiCGSTAB in `precision` */
+  int inner_iters;       /* GCR: inner iterations per step */
+  double inner_tol;      /* GCR: inner stop at |r| <= inner_tol |r_outer| */
+  int gcr_k;             /* GCR: directions kept before a restart (<= 16) */
 } qcuInvertParam;
 
 typedef struct {
   int iterations;
-  int reliable_updates;
+  int reliable_updates;  /* BiCGSTAB: reliable updates; GCR: outer steps */
   int status;            /* 1 converged, 2 max iterations, 3 breakdown, 4 NaN/Inf */
   int restarts;
   double true_residual;  /* ||b - M x|| / ||b||, recomputed in FP64 at the end */

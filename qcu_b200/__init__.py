@@ -72,6 +72,10 @@ class QcuInvertParam(ctypes.Structure):
         ("x0_seed", ctypes.c_ulonglong),
         ("use_clover", ctypes.c_int),
         ("chunk", ctypes.c_int),
+        ("solver", ctypes.c_int),
+        ("inner_iters", ctypes.c_int),
+        ("inner_tol", ctypes.c_double),
+        ("gcr_k", ctypes.c_int),
     ]
 
 
@@ -240,11 +244,18 @@ class Gauge:
 
     def invert(self, x, b, kappa: float, tol: float = 1e-10, maxiter: int = 10000, precision: int = 64,
                delta: float = 0.1, clover: bool = False, x0_mode: int = 0, x0_seed: int = 0, abs_tol: bool = False,
-               chunk: int = 0) -> dict:
+               chunk: int = 0, solver: str = "bicgstab", inner_iters: int = 16, inner_tol: float = 0.1,
+               gcr_k: int = 8) -> dict:
+        """Solve M x = b (full spinors).  solver="bicgstab": BiCGSTAB in
+        `precision` with FP64 reliable updates; solver="gcr": FP64 flexible
+        GCR(gcr_k) preconditioned by `inner_iters` BiCGSTAB iterations in
+        `precision` (or until the inner residual drops by inner_tol)."""
         p = QcuInvertParam()
         _lib.qcuInvertParamDefault(ctypes.byref(p))
         p.kappa, p.tol, p.maxiter, p.precision, p.delta = kappa, tol, maxiter, precision, delta
         p.abs_tol, p.x0_mode, p.x0_seed, p.use_clover, p.chunk = int(abs_tol), x0_mode, x0_seed, int(clover), chunk
+        p.solver = {"bicgstab": 0, "gcr": 1}[solver]
+        p.inner_iters, p.inner_tol, p.gcr_k = inner_iters, inner_tol, gcr_k
         r = QcuInvertResult()
         _check(_lib.qcuInvert(self._h, _ptr(x), _ptr(b), ctypes.byref(p), ctypes.byref(r)))
         return r.as_dict()

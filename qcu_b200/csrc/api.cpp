@@ -161,6 +161,10 @@ void qcuInvertParamDefault(qcuInvertParam *p) {
   p->x0_seed = d.x0_seed;
   p->use_clover = d.use_clover;
   p->chunk = d.chunk;
+  p->solver = d.solver;
+  p->inner_iters = d.inner_iters;
+  p->inner_tol = d.inner_tol;
+  p->gcr_k = d.gcr_k;
 }
 
 int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuInvertResult *r) {
@@ -177,6 +181,10 @@ int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuIn
   s.x0_seed = p->x0_seed;
   s.use_clover = p->use_clover;
   s.chunk = p->chunk;
+  s.solver = p->solver;
+  s.inner_iters = p->inner_iters;
+  s.inner_tol = p->inner_tol;
+  s.gcr_k = p->gcr_k;
   require(s.tol > 0, "tol must be positive");
   require(s.delta >= 0 && s.delta < 1, "delta must be in [0, 1)");
   SolveInfo info = solve(*h->h, x, b, s);

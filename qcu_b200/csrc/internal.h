@@ -98,7 +98,7 @@ struct Context {
   cudaStream_t stream = nullptr;
   SolverState *st = nullptr;       // device
   SolverState *st_host = nullptr;  // pinned mirror
-  double *partials = nullptr;      // MAX_REDUCE_BLOCKS * 8 doubles (dslash grids may exceed: sized dynamically)
+  double *partials = nullptr;      // blocks * RED_MAXV doubles (grown to the largest grid used)
   size_t partials_blocks = 0;
   std::mutex mu;
   void ensure_partials(size_t blocks);

@@ -13,6 +13,8 @@ namespace qcu {
 
 enum SolverStatus { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_BREAKDOWN = 3, ST_NAN = 4 };
 
+constexpr int RED_MAXV = 40;  // largest number of doubles one reduction produces (partials stride)
+
 struct SolverState {
   double rho[2], rho_prev[2], alpha[2], omega[2], beta[2];
   double rr;       // iterated ||r||^2 of the current inner residual
@@ -20,10 +22,11 @@ struct SolverState {
   double rr_true;  // last FP64 true ||r||^2
   double tol2;     // stop when the FP64 true ||r||^2 <= tol2
   double delta2;   // reliable update when rr <= delta2 * rr_max (0: only at the end)
-  double sums[8];  // result of the last FIN_STORE reduction
+  double inner_rel2;  // inner mode: stop when rr <= inner_rel2 * rr(start)
+  double sums[RED_MAXV];  // result of the last FIN_STORE reduction
   int iter, maxiter, done, update, status, nupdates;
+  int inner_mode;  // 1: a preconditioner solve (no reliable updates, stops on inner_rel2)
   unsigned ticket;
-  int pad;
 };
 
 // gate modes: which kernels of a captured iteration actually run
@@ -51,7 +54,7 @@ __device__ __forceinline__ bool bad_number(double v) { return !(v == v) || v > 1
 __device__ inline void finalize(SolverState *st, int op, const double *s) {
   switch (op) {
     case FIN_STORE:
-      for (int k = 0; k < 8; k++) st->sums[k] = s[k];
+      for (int k = 0; k < RED_MAXV; k++) st->sums[k] = s[k];
       break;
     case FIN_ALPHA: {
       Cpx<double> den(s[0], s[1]);
@@ -86,7 +89,12 @@ __device__ inline void finalize(SolverState *st, int op, const double *s) {
         st->status = ST_NAN;
         st->done = 1;
       } else if (s[2] <= st->tol2 || s[2] <= st->delta2 * st->rr_max) {
-        st->update = 1;  // fold x, recompute the FP64 true residual
+        if (st->inner_mode) {
+          st->status = ST_CONVERGED;
+          st->done = 1;
+        } else {
+          st->update = 1;  // fold x, recompute the FP64 true residual
+        }
       } else if (s[0] == 0.0 && s[1] == 0.0) {
         st->status = ST_BREAKDOWN;
         st->done = 1;
@@ -130,6 +138,9 @@ __device__ inline void finalize(SolverState *st, int op, const double *s) {
       st->rr_max = s[2];
       st->rr_true = s[2];
       st->update = 0;
+      st->iter = 0;
+      st->nupdates = 0;
+      if (st->inner_mode) st->tol2 = st->inner_rel2 * s[2];
       if (bad_number(s[2])) {
         st->status = ST_NAN;
         st->done = 1;
@@ -146,7 +157,7 @@ __device__ inline void finalize(SolverState *st, int op, const double *s) {
 
 struct RedCtx {
   SolverState *st;
-  double *partials;  // [gridDim.x][8]
+  double *partials;  // [gridDim.x][RED_MAXV]
   int op;
 };
 
@@ -188,7 +199,7 @@ __device__ __forceinline__ void grid_reduce(double v[NV], const RedCtx &rc) {
   block_sum<NV, BS>(v, part);
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int k = 0; k < NV; k++) rc.partials[(size_t)blockIdx.x * 8 + k] = part[k];
+    for (int k = 0; k < NV; k++) rc.partials[(size_t)blockIdx.x * RED_MAXV + k] = part[k];
     __threadfence();
     unsigned t = atomicAdd(&rc.st->ticket, 1u);
     last = (t == gridDim.x - 1);
@@ -201,14 +212,14 @@ __device__ __forceinline__ void grid_reduce(double v[NV], const RedCtx &rc) {
   for (int k = 0; k < NV; k++) acc[k] = 0.0;
   for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) {
 #pragma unroll
-    for (int k = 0; k < NV; k++) acc[k] += ((volatile double *)rc.partials)[(size_t)b * 8 + k];
+    for (int k = 0; k < NV; k++) acc[k] += ((volatile double *)rc.partials)[(size_t)b * RED_MAXV + k];
   }
   double tot[NV];
   block_sum<NV, BS>(acc, tot);
   if (threadIdx.x == 0) {
-    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double s[RED_MAXV];
 #pragma unroll
-    for (int k = 0; k < NV; k++) s[k] = tot[k];
+    for (int k = 0; k < RED_MAXV; k++) s[k] = k < NV ? tot[k] : 0.0;
     finalize(rc.st, rc.op, s);
     rc.st->ticket = 0;
     __threadfence();

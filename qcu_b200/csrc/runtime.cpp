@@ -92,7 +92,7 @@ void Context::ensure_partials(size_t blocks) {
   if (blocks <= partials_blocks) return;
   if (partials) cudaFree(partials);
   partials = nullptr;
-  QCU_CUDA(cudaMalloc(&partials, blocks * 8 * sizeof(double)));
+  QCU_CUDA(cudaMalloc(&partials, blocks * RED_MAXV * sizeof(double)));
   partials_blocks = blocks;
 }
 

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "gcr.h"
 #include "solver.h"
 
 namespace qcu {
@@ -176,11 +177,230 @@ static void enqueue_iteration(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs,
   launch_rconv(kind, Vh, vs, ctx, GATE_UPDATE, ctx.stream);
 }
 
+// Inner preconditioner solve of the GCR outer loop: BiCGSTAB in the inner
+// precision on M_pc z = r64, from zero, until |r| <= inner_tol |r64| or
+// inner_iters iterations.  The whole solve (init, iterations, conversion of the
+// result to FP64) is one captured graph, replayed once per GCR step: stopping
+// is decided on the device (gated launches), so the host never waits on it.
+static cudaGraphExec_t capture_inner_solve(Dsl &dP, Workspace &w, const VecSet &vs, double kappa, bool clov,
+                                           int iters, Spinor &z_out, long long &nodes) {
+  Context &ctx = dP.ctx;
+  const int Vh = dP.G.g.Vh, kind = dP.kind;
+  const double k2 = kappa * kappa;
+  cudaStream_t st = ctx.stream;
+  cudaGraph_t graph;
+  const long long before = launch_count();
+  QCU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  try {
+    launch_init(kind, Vh, vs, ctx, st);
+    for (int k = 0; k < iters; k++) {
+      launch_pupdate(kind, Vh, vs, ctx.st, GATE_NOT_DONE, st);
+      dP(0, w.p, w.tmp, clov, 1.0, nullptr, 0, nullptr, 0, RED_NONE, FIN_STORE, nullptr, GATE_NOT_DONE);
+      dP(1, w.tmp, w.v, clov, -k2, &w.p, 1.0, nullptr, 0, RED_DOT_RT, FIN_ALPHA, &w.rt, GATE_NOT_DONE);
+      launch_supdate(kind, Vh, vs, ctx.st, GATE_NOT_DONE, st);
+      dP(0, w.s, w.tmp, clov, 1.0, nullptr, 0, nullptr, 0, RED_NONE, FIN_STORE, nullptr, GATE_NOT_DONE);
+      dP(1, w.tmp, w.t, clov, -k2, &w.s, 1.0, nullptr, 0, RED_TS_TT, FIN_OMEGA, nullptr, GATE_NOT_DONE);
+      launch_xrupdate(kind, Vh, vs, ctx, GATE_NOT_DONE, st);
+    }
+    launch_convert(w.x.kind, SOA64, Vh, w.x.data.p, w.x.norm.as<float>(), z_out.data.p, nullptr, st);
+  } catch (...) {
+    cudaStreamEndCapture(st, &graph);
+    throw;
+  }
+  QCU_CUDA(cudaStreamEndCapture(st, &graph));
+  nodes = launch_count() - before;
+  set_launch_count(before);
+  cudaGraphExec_t exec;
+  QCU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+  QCU_CUDA(cudaGraphDestroy(graph));
+  return exec;
+}
+
+namespace {
+struct GcrSpace {
+  Spinor W[GCR_MAXK], Z[GCR_MAXK], znew, wnew;
+  void prepare(int m, int Vh) {
+    for (int j = 0; j < m; j++) {
+      W[j].alloc(SOA64, Vh);
+      Z[j].alloc(SOA64, Vh);
+    }
+    znew.alloc(SOA64, Vh);
+    wnew.alloc(SOA64, Vh);
+  }
+};
+GcrSpace &gcr_space() {
+  static GcrSpace *g = new GcrSpace();  // intentionally never destroyed
+  return *g;
+}
+}  // namespace
+
+// Flexible GCR(m) on M_pc in FP64 with the inner solve above as right
+// preconditioner: x64/r64 advance until the recursive |r|^2 <= tol2.
+static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const SolveParams &prm, double tol2,
+                    SolveInfo &info) {
+  Context &ctx = dP.ctx;
+  const int Vh = dP.G.g.Vh;
+  const bool clov = prm.use_clover != 0;
+  const double kappa = prm.kappa, k2 = kappa * kappa;
+  const int m = std::max(1, std::min(prm.gcr_k, GCR_MAXK));
+  cudaStream_t st = ctx.stream;
+  GcrSpace &gs = gcr_space();
+  gs.prepare(m, Vh);
+  // inner solver settings stay constant across the GCR steps
+  SolverState init{};
+  init.inner_mode = 1;
+  init.inner_rel2 = prm.inner_tol * prm.inner_tol;
+  init.maxiter = prm.inner_iters;
+  *ctx.st_host = init;
+  QCU_CUDA(cudaMemcpyAsync(ctx.st, ctx.st_host, sizeof(SolverState), cudaMemcpyHostToDevice, st));
+  long long nodes = 0;
+  cudaGraphExec_t inner = capture_inner_solve(dP, w, vs, kappa, clov, prm.inner_iters, gs.znew, nodes);
+  GcrArgs a;
+  a.w = gs.wnew.data.p;
+  a.z = gs.znew.data.p;
+  for (int j = 0; j < m; j++) {
+    a.W[j] = gs.W[j].data.p;
+    a.Z[j] = gs.Z[j].data.p;
+  }
+  a.x = w.x64.data.p;
+  a.r = w.r64.data.p;
+  double nw[GCR_MAXK] = {};  // |W_j|^2
+  try {
+    while (info.iterations < prm.maxiter) {
+      // true residual at the start of every cycle
+      d64(0, w.x64, w.tmp64, clov, 1.0);
+      d64(1, w.tmp64, w.r64, clov, k2, &w.bp, 1.0, &w.x64, -1.0, RED_NORM, FIN_STORE);
+      double rr = read_state(ctx).sums[0];
+      if (!(rr == rr)) {
+        info.status = ST_NAN;
+        break;
+      }
+      if (rr <= tol2) {
+        info.status = ST_CONVERGED;
+        break;
+      }
+      for (int k = 0; k < m && rr > tol2 && info.iterations < prm.maxiter; k++) {
+        QCU_CUDA(cudaGraphLaunch(inner, st));
+        note_launch(nodes);
+        // w = M_pc z
+        d64(0, gs.znew, w.tmp64, clov, 1.0);
+        d64(1, w.tmp64, gs.wnew, clov, -k2, &gs.znew, 1.0);
+        a.k = k;
+        if (k > 0) {
+          launch_gcr_multidot(Vh, a, ctx, st);
+          const SolverState S = read_state(ctx);
+          for (int j = 0; j < k; j++) {
+            // |W_j|^2 was stored when W_j was made
+            a.beta[2 * j] = S.sums[2 * j] / nw[j];
+            a.beta[2 * j + 1] = S.sums[2 * j + 1] / nw[j];
+          }
+          info.iterations += S.iter;  // inner iterations of this step
+        } else {
+          info.iterations += read_state(ctx).iter;
+        }
+        launch_gcr_orth(Vh, a, ctx, st);
+        SolverState S = read_state(ctx);
+        const double ww = S.sums[0];
+        if (!(ww > 0.0) || !(ww < 1e300)) {
+          info.status = ww == ww ? ST_BREAKDOWN : ST_NAN;
+          rr = -1;
+          break;
+        }
+        nw[k] = ww;
+        a.alpha[0] = S.sums[1] / ww;
+        a.alpha[1] = S.sums[2] / ww;
+        launch_gcr_update(Vh, a, ctx, st);
+        rr = read_state(ctx).sums[0];
+        info.iter_residual2 = rr;
+        info.updates++;  // outer (FP64) steps
+      }
+      if (rr < 0) break;
+    }
+  } catch (...) {
+    cudaGraphExecDestroy(inner);
+    throw;
+  }
+  cudaGraphExecDestroy(inner);
+  if (info.status == ST_RUNNING && info.iterations >= prm.maxiter) info.status = ST_MAXITER;
+}
+
+// BiCGSTAB on M_pc in the inner precision with reliable updates; x64 advances
+// until the FP64 true |r|^2 <= tol2 (or a stop condition).  Returns the state.
+static SolverState run_bicgstab(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const SolveParams &prm, double tol2,
+                                int maxiter) {
+  Context &ctx = dP.ctx;
+  const int Vh = dP.G.g.Vh, kind = dP.kind;
+  const bool clov = prm.use_clover != 0;
+  const double kappa = prm.kappa;
+  cudaStream_t st = ctx.stream;
+  const int chunk = prm.chunk > 0 ? prm.chunk : (Vh >= (1 << 18) ? 8 : (Vh >= (1 << 14) ? 16 : 32));
+  const bool use_graph = getenv("QCU_NO_GRAPH") == nullptr;
+  // r64 = b' - M_pc x64
+  d64(0, w.x64, w.tmp64, clov, 1.0);
+  d64(1, w.tmp64, w.r64, clov, kappa * kappa, &w.bp, 1.0, &w.x64, -1.0, RED_NORM, FIN_RTRUE);
+  SolverState init{};
+  init.tol2 = tol2;
+  init.delta2 = prm.delta * prm.delta;
+  init.maxiter = maxiter;
+  *ctx.st_host = init;
+  QCU_CUDA(cudaMemcpyAsync(ctx.st, ctx.st_host, sizeof(SolverState), cudaMemcpyHostToDevice, st));
+  launch_init(kind, Vh, vs, ctx, st);
+  SolverState S = read_state(ctx);
+  if (!S.done) {
+    cudaGraphExec_t exec = nullptr;
+    long long nodes = 0;
+    if (use_graph) {
+      cudaGraph_t graph;
+      const long long before = launch_count();
+      QCU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        for (int k = 0; k < chunk; k++) enqueue_iteration(dP, d64, w, vs, kappa, clov);
+      } catch (...) {
+        cudaStreamEndCapture(st, &graph);
+        throw;
+      }
+      QCU_CUDA(cudaStreamEndCapture(st, &graph));
+      nodes = launch_count() - before;  // captured, not run: counted per replay below
+      set_launch_count(before);
+      QCU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+      QCU_CUDA(cudaGraphDestroy(graph));
+    }
+    // every iteration advances st->iter, and the iteration that reaches
+    // maxiter sets done, so this loop ends after at most maxiter/chunk + 1
+    // passes; the cap below only guards against a logic error
+    const long long max_passes = (long long)maxiter / chunk + 8;
+    try {
+      for (long long pass = 0;; pass++) {
+        require(pass < max_passes, "solver did not terminate within maxiter (internal error)");
+        if (exec) {
+          QCU_CUDA(cudaGraphLaunch(exec, st));
+          note_launch(nodes);
+        } else {
+          for (int k = 0; k < chunk; k++) enqueue_iteration(dP, d64, w, vs, kappa, clov);
+        }
+        S = read_state(ctx);
+        if (S.done) break;
+      }
+    } catch (...) {
+      if (exec) cudaGraphExecDestroy(exec);
+      throw;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+  // fold whatever the inner solution still holds (after a NaN the inner
+  // partial solution is discarded: x64 is the last good FP64 iterate)
+  if (S.status != ST_NAN) launch_xfold(w.x.kind, Vh, vs, ctx.st, GATE_ALWAYS, st);
+  return S;
+}
+
 SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParams &prm) {
   require(x_pyq != nullptr && b_pyq != nullptr, "solve: null spinor pointer");
   require(prm.kappa > 0, "solve: kappa must be positive");
   require(prm.maxiter > 0, "solve: maxiter must be positive");
   require(!prm.use_clover || G.has_clover, "solve: clover requested but the gauge handle has no clover term");
+  require(prm.solver == 0 || prm.solver == 1, "solve: solver must be 0 (BiCGSTAB) or 1 (GCR)");
+  require(prm.solver == 0 || (prm.inner_iters > 0 && prm.gcr_k > 0 && !prm.abs_tol),
+          "solve: GCR needs inner_iters > 0, gcr_k > 0 and a relative tolerance");
   const auto t0 = std::chrono::steady_clock::now();
   Context &ctx = context();
   std::lock_guard<std::mutex> lk(ctx.mu);
@@ -225,69 +445,22 @@ SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParam
   else QCU_CUDA(cudaMemsetAsync(w.x64.data.p, 0, spinor_bytes(SOA64, Vh), st));
 
   const VecSet vs = make_vecset(w);
-  int chunk = prm.chunk > 0 ? prm.chunk : (Vh >= (1 << 18) ? 8 : (Vh >= (1 << 14) ? 16 : 32));
-  const bool use_graph = getenv("QCU_NO_GRAPH") == nullptr;
-  int total_iter = 0, total_updates = 0;
-  SolverState S{};
   for (int restart = 0;; restart++) {
-    // r64 = b' - M_pc x64
-    d64(0, w.x64, w.tmp64, clov, 1.0);
-    d64(1, w.tmp64, w.r64, clov, kappa * kappa, &w.bp, 1.0, &w.x64, -1.0, RED_NORM, FIN_RTRUE);
-    SolverState init{};
-    init.tol2 = tol2;
-    init.delta2 = prm.delta * prm.delta;
-    init.maxiter = prm.maxiter - total_iter;
-    *ctx.st_host = init;
-    QCU_CUDA(cudaMemcpyAsync(ctx.st, ctx.st_host, sizeof(SolverState), cudaMemcpyHostToDevice, st));
-    launch_init(kind, Vh, vs, ctx, st);
-    S = read_state(ctx);
-    if (!S.done) {
-      cudaGraphExec_t exec = nullptr;
-      long long nodes = 0;
-      if (use_graph) {
-        cudaGraph_t graph;
-        const long long before = launch_count();
-        QCU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        try {
-          for (int k = 0; k < chunk; k++) enqueue_iteration(dP, d64, w, vs, kappa, clov);
-        } catch (...) {
-          cudaStreamEndCapture(st, &graph);
-          throw;
-        }
-        QCU_CUDA(cudaStreamEndCapture(st, &graph));
-        nodes = launch_count() - before;  // captured, not run: counted per replay below
-        set_launch_count(before);
-        QCU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-        QCU_CUDA(cudaGraphDestroy(graph));
+    if (prm.solver == 1) {
+      info.status = ST_RUNNING;
+      run_gcr(dP, d64, w, vs, prm, tol2, info);
+    } else {
+      const SolverState S = run_bicgstab(dP, d64, w, vs, prm, tol2, prm.maxiter - info.iterations);
+      info.iterations += S.iter;
+      info.updates += S.nupdates;
+      info.status = S.status;
+      info.iter_residual2 = S.rr;
+      // BiCGSTAB breakdown (rho, <rt,v> or <t,t> vanishing) or a non-finite
+      // inner value: restart from the FP64 iterate with a fresh shadow residual
+      if ((S.status == ST_BREAKDOWN || S.status == ST_NAN) && info.restarts < 8 && info.iterations < prm.maxiter) {
+        info.restarts++;
+        continue;
       }
-      // every iteration advances st->iter, and the iteration that reaches
-      // maxiter sets done, so this loop ends after at most maxiter/chunk + 1
-      // passes; the cap below only guards against a logic error
-      const long long max_passes = (long long)init.maxiter / chunk + 8;
-      for (long long pass = 0;; pass++) {
-        require(pass < max_passes, "solver did not terminate within maxiter (internal error)");
-        if (exec) {
-          QCU_CUDA(cudaGraphLaunch(exec, st));
-          note_launch(nodes);
-        } else
-          for (int k = 0; k < chunk; k++) enqueue_iteration(dP, d64, w, vs, kappa, clov);
-        S = read_state(ctx);
-        if (S.done) break;
-      }
-      if (exec) cudaGraphExecDestroy(exec);
-    }
-    // fold whatever the inner solution still holds (after a NaN the inner
-    // partial solution is discarded: x64 is the last good FP64 iterate)
-    if (S.status != ST_NAN) launch_xfold(w.x.kind, Vh, vs, ctx.st, GATE_ALWAYS, st);
-    total_iter += S.iter;
-    total_updates += S.nupdates;
-    info.status = S.status;
-    info.iter_residual2 = S.rr;
-    // BiCGSTAB breakdown (rho, <rt,v> or <t,t> vanishing) or a non-finite
-    // inner value: restart from the FP64 iterate with a fresh shadow residual
-    if ((S.status == ST_BREAKDOWN || S.status == ST_NAN) && info.restarts < 8 && total_iter < prm.maxiter) {
-      info.restarts++;
-      continue;
     }
     // x_e = A_e^-1 (b_e + kappa D_eo x_o)
     d64(0, w.x64, w.tmp64, false, kappa, &w.be, 1.0);
@@ -308,16 +481,14 @@ SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParam
     }
     info.true_residual = std::sqrt(rr / bb);
     const bool relative_ok = prm.abs_tol || info.true_residual <= prm.tol;
-    if (S.status != ST_CONVERGED || relative_ok || restart >= 12 || total_iter >= prm.maxiter) {
-      if (S.status == ST_CONVERGED && !relative_ok) info.status = ST_MAXITER;
+    if (info.status != ST_CONVERGED || relative_ok || restart >= 12 || info.iterations >= prm.maxiter) {
+      if (info.status == ST_CONVERGED && !relative_ok) info.status = ST_MAXITER;
       break;
     }
     // the preconditioned residual met tol2 but the full one did not: tighten and resume from x64
     tol2 *= 0.25 * (prm.tol * prm.tol * bb) / std::max(rr, 1e-300);
     info.restarts++;
   }
-  info.iterations = total_iter;
-  info.updates = total_updates;
   launch_convert(SOA64, AOS64, Vh, w.xe.data.p, nullptr, xp, nullptr, st);
   launch_convert(SOA64, AOS64, Vh, w.x64.data.p, nullptr, xp + half, nullptr, st);
   QCU_CUDA(cudaStreamSynchronize(st));

@@ -36,11 +36,15 @@ struct SolveParams {
   uint64_t x0_seed = 0;
   int use_clover = 0;
   int chunk = 0;            // iterations per captured graph (0: automatic)
+  int solver = 0;           // 0 BiCGSTAB (reliable updates), 1 flexible GCR with an inner BiCGSTAB
+  int inner_iters = 16;     // GCR: iterations of the inner solve per step
+  double inner_tol = 0.1;   // GCR: inner solve stops at |r| <= inner_tol |r_outer|
+  int gcr_k = 8;            // GCR: directions kept before a restart (<= 16)
 };
 
 struct SolveInfo {
   int iterations = 0;
-  int updates = 0;
+  int updates = 0;           // BiCGSTAB: reliable updates; GCR: outer steps
   int status = 0;
   int restarts = 0;
   double true_residual = 0;  // ||b - M x|| / ||b||, FP64, full two-parity system

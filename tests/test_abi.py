@@ -60,13 +60,13 @@ def test_struct_layouts_match_header(tmp_path):
     src.write_text(
         "#include <stdio.h>\n#include <stddef.h>\n#include \"qcu.h\"\n#include \"qcu_ext.h\"\n"
         "int main(void){printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(QcuParam), sizeof(qcuInvertParam),"
-        " offsetof(qcuInvertParam, x0_seed), offsetof(qcuInvertParam, chunk), sizeof(qcuInvertResult),"
+        " offsetof(qcuInvertParam, x0_seed), offsetof(qcuInvertParam, inner_tol), sizeof(qcuInvertResult),"
         " offsetof(qcuInvertResult, seconds)); return 0;}\n")
     exe = tmp_path / "layout"
     subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     assert got == [ctypes.sizeof(q.QcuParam), ctypes.sizeof(q.QcuInvertParam), q.QcuInvertParam.x0_seed.offset,
-                   q.QcuInvertParam.chunk.offset, ctypes.sizeof(q.QcuInvertResult),
+                   q.QcuInvertParam.inner_tol.offset, ctypes.sizeof(q.QcuInvertResult),
                    q.QcuInvertResult.seconds.offset]
 
 

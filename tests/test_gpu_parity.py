@@ -208,3 +208,24 @@ def test_invert_maxiter_reports_status(q):
         info = G.invert(x, dev(b), 0.124, tol=1e-12, maxiter=3)
     assert info["status"] == 2 and info["iterations"] == 3
     assert np.isfinite(host(x)).all()
+
+
+@pytest.mark.parametrize("prec", [32, 16])
+@pytest.mark.parametrize("clover", [False, True])
+def test_invert_gcr_true_residual(q, prec, clover):
+    """Flexible GCR (FP64) preconditioned by a low-precision inner BiCGSTAB."""
+    latt = [8, 8, 8, 16]
+    U = O.gauge_smooth(latt, 0.25, 10)
+    b = O.fermion_gauss(O.full_shape(latt), 20)
+    kappa = 0.126
+    c = kappa * 1.0
+    A = [O.clover_build(U, latt, p, c) for p in (0, 1)] if clover else [None, None]
+    with q.Gauge(dev(U), latt, t_boundary=-1.0, clover_coeff=c if clover else 0.0) as G:
+        x = empty_like_dev(O.full_shape(latt))
+        info = G.invert(x, dev(b), kappa, tol=1e-10, maxiter=5000, precision=prec, clover=clover, solver="gcr",
+                        inner_iters=12, gcr_k=6)
+    assert info["status"] == 1, info
+    assert info["true_residual"] <= 1e-10
+    r = b - O.mfull(host(x), U, latt, kappa, -1.0, True, A[0], A[1])
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05e-10
+    assert info["reliable_updates"] >= 2  # outer steps
