@@ -40,7 +40,7 @@ PLAIN_ITERS_REF = 1000    # iteration count used to extrapolate the CPU sample w
 TOL = 1e-10
 METRIC = "solve s to 1e-10 true residual, chosen vs plain FP64, 1 B200; dslash HBM GB/s"
 # algorithmic bytes per output site of the hopping term (in-spinor + 8 recon-12 links + out-spinor)
-DSLASH_BYTES = {64: 192 + 8 * 96 + 192, 32: 96 + 8 * 48 + 96, 16: 52 + 8 * 24 + 52}
+DSLASH_BYTES = {"64": 192 + 8 * 96 + 192, "32": 96 + 8 * 48 + 96, "16": 52 + 8 * 24 + 52, "32/16": 96 + 8 * 24 + 96}
 DSLASH_FLOPS = 1320
 
 
@@ -50,7 +50,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", type=int, default=32, choices=[16, 32, 64], help="inner precision of the chosen solver")
+    ap.add_argument("--precision", type=int, default=16, choices=[16, 32, 64], help="inner precision of the chosen solver")
+    ap.add_argument("--solver", default="gcr", choices=["gcr", "bicgstab"], help="chosen solver")
+    ap.add_argument("--gauge-precision", type=int, default=0, choices=[0, 16], help="16: FP32 spinors with 16-bit links")
+    ap.add_argument("--inner-iters", type=int, default=64)
+    ap.add_argument("--inner-tol", type=float, default=0.05)
+    ap.add_argument("--gcr-k", type=int, default=4)
     ap.add_argument("--kappa", type=float, default=KAPPA)
     ap.add_argument("--latt", type=int, nargs=4, default=LATT)
     ap.add_argument("--no-e2e", action="store_true")
@@ -217,10 +222,13 @@ def run_ours(args, world, rank, local, pg):
     G = q.Gauge(gauge, latt, t_boundary=T_BC)
     lib_stream = torch.cuda.ExternalStream(q.stream_handle(), device=dev)
 
-    def timed_solve(prec, delta):
+    chosen_kw = dict(precision=args.precision, delta=0.1, solver=args.solver, inner_iters=args.inner_iters,
+                     inner_tol=args.inner_tol, gcr_k=args.gcr_k, gauge_precision=args.gauge_precision)
+
+    def timed_solve(**kw):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(lib_stream)
-        info = G.invert(x, b, args.kappa, tol=TOL, maxiter=20000, precision=prec, delta=delta)
+        info = G.invert(x, b, args.kappa, tol=TOL, maxiter=20000, **kw)
         e1.record(lib_stream)
         e1.synchronize()
         if info["status"] != 1 or info["true_residual"] > TOL:
@@ -228,11 +236,11 @@ def run_ours(args, world, rank, local, pg):
         return e0.elapsed_time(e1) / 1e3, info
 
     # plain FP64 BiCGSTAB (reliable update only at the end = true-residual check)
-    plain_t, plain_info = timed_solve(64, 0.0)
-    plain_t = min(plain_t, timed_solve(64, 0.0)[0])
+    plain_t, plain_info = timed_solve(precision=64, delta=0.0)
+    plain_t = min(plain_t, timed_solve(precision=64, delta=0.0)[0])
     # chosen solver: warm-up then K timed solves
     for _ in range(args.warmup):
-        timed_solve(args.precision, 0.1)
+        timed_solve(**chosen_kw)
     if pg is not None:
         pg.barrier()
     torch.cuda.synchronize()
@@ -243,7 +251,7 @@ def run_ours(args, world, rank, local, pg):
     e0.record(lib_stream)
     infos = []
     for _ in range(args.steps):
-        infos.append(G.invert(x, b, args.kappa, tol=TOL, maxiter=20000, precision=args.precision, delta=0.1))
+        infos.append(G.invert(x, b, args.kappa, tol=TOL, maxiter=20000, **chosen_kw))
     e1.record(lib_stream)
     e1.synchronize()
     torch.cuda.synchronize()
@@ -260,15 +268,16 @@ def run_ours(args, world, rank, local, pg):
     pk, pk_kind = peaks()
     vh = L.vh
     dsl = {}
-    for prec in (64, 32, 16):
-        ms = G.bench_dslash(prec, False, 50)
-        dsl[prec] = {"ms": ms, "GBps": DSLASH_BYTES[prec] * vh / (ms * 1e-3) / 1e9,
-                     "TFLOPs": DSLASH_FLOPS * vh / (ms * 1e-3) / 1e12}
-    dom = dsl[args.precision]
+    for key, (prec, gprec) in {"64": (64, 0), "32": (32, 0), "16": (16, 0), "32/16": (32, 16)}.items():
+        ms = G.bench_dslash(prec, False, 50, gauge_precision=gprec)
+        dsl[key] = {"ms": ms, "GBps": DSLASH_BYTES[key] * vh / (ms * 1e-3) / 1e9,
+                    "TFLOPs": DSLASH_FLOPS * vh / (ms * 1e-3) / 1e12}
+    key = f"{args.precision}/16" if args.gauge_precision == 16 else str(args.precision)
+    dom = dsl[key]
+    kname = {"64": "SOA64,GSOA64", "32": "SOA32,GSOA32", "16": "SOA16,GSOA16", "32/16": "SOA32,GSOA16"}[key]
     roofline = {"bound": "hbm", "achieved": round(dom["GBps"], 1), "peak": pk, "unit": "GB/s",
                 "frac": round(dom["GBps"] / pk, 4), "traffic": None,
-                "kernel": f"k_dslash<{ {64: 'SOA64', 32: 'SOA32', 16: 'SOA16'}[args.precision] }> "
-                          f"({DSLASH_BYTES[args.precision]} B/site x {vh} sites per launch)",
+                "kernel": f"k_dslash<{kname}> ({DSLASH_BYTES[key]} B/site x {vh} sites per launch)",
                 "peak_kind": pk_kind}
 
     # end to end through the C ABI with host buffers: H2D gauge + b, load, solve, D2H x
@@ -288,7 +297,7 @@ def run_ours(args, world, rank, local, pg):
             dg.copy_(hg, non_blocking=True)
             db.copy_(hb, non_blocking=True)
             with q.Gauge(dg, latt, t_boundary=T_BC) as G2:
-                info = G2.invert(dx, db, args.kappa, tol=TOL, maxiter=20000, precision=args.precision, delta=0.1)
+                info = G2.invert(dx, db, args.kappa, tol=TOL, maxiter=20000, **chosen_kw)
             hx.copy_(dx, non_blocking=True)
             s1.record()
             s1.synchronize()
@@ -311,19 +320,23 @@ def run_ours(args, world, rank, local, pg):
             "metric": METRIC, "value": round(per_solve, 4), "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(per_solve * 1e3, 2), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": {64: "f64", 32: "f32 storage / f64 reductions", 16: "int16+norm storage / f32 math / f64 reductions"}[
-                args.precision],
+            "dtype": ({64: "f64", 32: "f32 storage / f64 reductions", 16: "int16+norm storage / f32 math / f64 reductions"}[
+                args.precision] + (" / int16 links" if args.gauge_precision == 16 else "") + " (outer FP64)"),
             "data": "synthetic (seeded smooth SU(3) gauge, Gaussian source)",
             "config": {"workload": "wilson-bicgstab-32^3x64-smooth-eps0.25", "latt": latt, "kappa": args.kappa,
-                       "tol": TOL, "t_boundary": T_BC, "solver": f"BiCGSTAB inner {args.precision}-bit, FP64 reliable updates (delta 0.1)",
+                       "tol": TOL, "t_boundary": T_BC,
+                       "solver": (f"FP64 flexible GCR({args.gcr_k}), inner BiCGSTAB {args.precision}-bit"
+                                  f"{'/16-bit links' if args.gauge_precision == 16 else ''} x{args.inner_iters} "
+                                  f"(inner tol {args.inner_tol})") if args.solver == "gcr" else
+                                 f"BiCGSTAB {args.precision}-bit, FP64 reliable updates (delta 0.1)",
                        "parallelism": "replicas" if world > 1 else "single", "l2": "working set (GBs) larger than L2"},
-            "chosen": {"iterations": chosen["iterations"], "reliable_updates": chosen["reliable_updates"],
+            "chosen": {"iterations": chosen["iterations"], "outer_steps_or_updates": chosen["reliable_updates"],
                        "true_residual": chosen["true_residual"]},
             "plain_fp64": {"seconds": round(plain_t, 4), "iterations": plain_info["iterations"],
                            "true_residual": plain_info["true_residual"]},
             "speedup_vs_plain_fp64": round(plain_t / per_solve, 3),
-            "dslash": {str(k): {"ms": round(v["ms"], 4), "GBps": round(v["GBps"], 1), "frac_of_peak": round(v["GBps"] / pk, 4),
-                                "TFLOPs": round(v["TFLOPs"], 2)} for k, v in dsl.items()},
+            "dslash": {k: {"ms": round(v["ms"], 4), "GBps": round(v["GBps"], 1), "frac_of_peak": round(v["GBps"] / pk, 4),
+                           "TFLOPs": round(v["TFLOPs"], 2)} for k, v in dsl.items()},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

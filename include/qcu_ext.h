@@ -63,6 +63,8 @@ typedef struct {
   int inner_iters;       /* GCR: inner iterations per step */
   double inner_tol;      /* GCR: inner stop at |r| <= inner_tol |r_outer| */
   int gcr_k;             /* GCR: directions kept before a restart (<= 16) */
+  int gauge_precision;   /* 0: links stored like the spinors; 16 (with precision 32): FP32
+                            spinors and 16-bit links in the inner operator */
 } qcuInvertParam;
 
 typedef struct {
@@ -109,10 +111,11 @@ long long qcuKernelLaunches(void);
 void *qcuGetStream(void);
 
 /* Kernel timing: `iters` back-to-back applications of the internal-layout
- * hopping term (precision 64/32/16, optionally with the clover inverse) on
- * random input, alternating parities, timed with CUDA events on the library
- * stream.  Returns the mean milliseconds per application. */
-int qcuBenchDslash(qcuGauge h, int precision, int use_clover, int iters, double *ms_per_call);
+ * hopping term (spinor precision 64/32/16, link precision 0 = same or 16 with
+ * FP32 spinors, optionally with the clover inverse) on random input,
+ * alternating parities, timed with CUDA events on the library stream.
+ * Returns the mean milliseconds per application. */
+int qcuBenchDslash(qcuGauge h, int precision, int gauge_precision, int use_clover, int iters, double *ms_per_call);
 
 #ifdef __cplusplus
 }

@@ -76,6 +76,7 @@ class QcuInvertParam(ctypes.Structure):
         ("inner_iters", ctypes.c_int),
         ("inner_tol", ctypes.c_double),
         ("gcr_k", ctypes.c_int),
+        ("gauge_precision", ctypes.c_int),
     ]
 
 
@@ -121,7 +122,8 @@ _lib.dslashCloverQcuNoAlloc.argtypes = [_vp, _vp, _vp, _P, ctypes.c_int]
 _lib.dslashCloverQcuNoAlloc.restype = ctypes.c_int
 _lib.qcuNoAllocMaxSites.restype = ctypes.c_int
 _lib.qcuKernelLaunches.restype = ctypes.c_longlong
-_lib.qcuBenchDslash.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+_lib.qcuBenchDslash.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_double)]
 
 
 class QcuError(RuntimeError):
@@ -245,7 +247,7 @@ class Gauge:
     def invert(self, x, b, kappa: float, tol: float = 1e-10, maxiter: int = 10000, precision: int = 64,
                delta: float = 0.1, clover: bool = False, x0_mode: int = 0, x0_seed: int = 0, abs_tol: bool = False,
                chunk: int = 0, solver: str = "bicgstab", inner_iters: int = 16, inner_tol: float = 0.1,
-               gcr_k: int = 8) -> dict:
+               gcr_k: int = 8, gauge_precision: int = 0) -> dict:
         """Solve M x = b (full spinors).  solver="bicgstab": BiCGSTAB in
         `precision` with FP64 reliable updates; solver="gcr": FP64 flexible
         GCR(gcr_k) preconditioned by `inner_iters` BiCGSTAB iterations in
@@ -256,13 +258,15 @@ class Gauge:
         p.abs_tol, p.x0_mode, p.x0_seed, p.use_clover, p.chunk = int(abs_tol), x0_mode, x0_seed, int(clover), chunk
         p.solver = {"bicgstab": 0, "gcr": 1}[solver]
         p.inner_iters, p.inner_tol, p.gcr_k = inner_iters, inner_tol, gcr_k
+        p.gauge_precision = gauge_precision
         r = QcuInvertResult()
         _check(_lib.qcuInvert(self._h, _ptr(x), _ptr(b), ctypes.byref(p), ctypes.byref(r)))
         return r.as_dict()
 
-    def bench_dslash(self, precision: int = 64, clover: bool = False, iters: int = 20) -> float:
+    def bench_dslash(self, precision: int = 64, clover: bool = False, iters: int = 20, gauge_precision: int = 0) -> float:
         ms = ctypes.c_double(0)
-        _check(_lib.qcuBenchDslash(self._h, int(precision), int(clover), int(iters), ctypes.byref(ms)))
+        _check(_lib.qcuBenchDslash(self._h, int(precision), int(gauge_precision), int(clover), int(iters),
+                                   ctypes.byref(ms)))
         return ms.value
 
 

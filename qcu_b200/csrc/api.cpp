@@ -165,6 +165,7 @@ void qcuInvertParamDefault(qcuInvertParam *p) {
   p->inner_iters = d.inner_iters;
   p->inner_tol = d.inner_tol;
   p->gcr_k = d.gcr_k;
+  p->gauge_precision = d.gauge_precision;
 }
 
 int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuInvertResult *r) {
@@ -185,6 +186,7 @@ int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuIn
   s.inner_iters = p->inner_iters;
   s.inner_tol = p->inner_tol;
   s.gcr_k = p->gcr_k;
+  s.gauge_precision = p->gauge_precision;
   require(s.tol > 0, "tol must be positive");
   require(s.delta >= 0 && s.delta < 1, "delta must be in [0, 1)");
   SolveInfo info = solve(*h->h, x, b, s);
@@ -242,13 +244,17 @@ void *qcuGetStream(void) {
   }
 }
 
-int qcuBenchDslash(qcuGauge h, int precision, int use_clover, int iters, double *ms_per_call) {
+int qcuBenchDslash(qcuGauge h, int precision, int gauge_precision, int use_clover, int iters, double *ms_per_call) {
   QCU_API_BEGIN
   require(h != nullptr && ms_per_call != nullptr && iters > 0, "bad arguments");
   GaugeHandle &G = *h->h;
   require(!use_clover || G.has_clover, "no clover term loaded");
   const int kind = precision == 64 ? SOA64 : precision == 32 ? SOA32 : precision == 16 ? SOA16 : -1;
   require(kind >= 0, "precision must be 64, 32 or 16");
+  if (gauge_precision == 0) gauge_precision = precision;
+  const int gkind = gauge_precision == 64 ? GSOA64 : gauge_precision == 32 ? GSOA32 : gauge_precision == 16 ? GSOA16 : -1;
+  require(gkind == (kind == SOA64 ? GSOA64 : kind == SOA32 ? GSOA32 : GSOA16) || (kind == SOA32 && gkind == GSOA16),
+          "unsupported spinor/link precision pair");
   Context &ctx = context();
   std::lock_guard<std::mutex> lk(ctx.mu);
   const int Vh = G.g.Vh;
@@ -261,7 +267,7 @@ int qcuBenchDslash(qcuGauge h, int precision, int use_clover, int iters, double 
   launch_convert(AOS64, kind, Vh, tmp.p, nullptr, a.data.p, a.norm.as<float>(), ctx.stream);
   launch_convert(AOS64, kind, Vh, tmp.p, nullptr, b.data.p, b.norm.as<float>(), ctx.stream);
   DslashArgs d;
-  d.gauge = G.gauge(kind);
+  d.gauge = gkind == GSOA64 ? G.g64.p : (gkind == GSOA32 ? G.g32.p : G.g16.p);
   d.t_bc = G.t_bc;
   d.a = 1.0;
   auto run = [&](int i) {
@@ -274,8 +280,7 @@ int qcuBenchDslash(qcuGauge h, int precision, int use_clover, int iters, double 
     d.out_norm = out.norm.as<float>();
     d.parity = par;
     d.clover = use_clover ? G.clover_inv(kind, par) : nullptr;
-    launch_dslash(kind, kind == SOA64 ? GSOA64 : kind == SOA32 ? GSOA32 : GSOA16, kind == SOA64 ? CSOA64 : CSOA32,
-                  G.g, d, ctx, ctx.stream);
+    launch_dslash(kind, gkind, kind == SOA64 ? CSOA64 : CSOA32, G.g, d, ctx, ctx.stream);
   };
   for (int i = 0; i < 3; i++) run(i);
   cudaEvent_t e0, e1;

@@ -129,15 +129,15 @@ __device__ void clover_leaves(const GaugeView<GAOS64> &U, const Geom &g, const i
 
 __device__ __forceinline__ C unit(int re, int im) { return C((double)re, (double)im); }
 
-// packed block store: d[0..5] then lower triangle
-__device__ __forceinline__ void block_store(void *out, int Vh, int blk, int s, const C M[36]) {
-  double2 *p = static_cast<double2 *>(out) + (size_t)blk * 18 * Vh + s;
+// packed block store (site-blocked CSOA64): d[0..5] then lower triangle
+__device__ __forceinline__ void block_store(void *out, int blk, int s, const C M[36]) {
+  double2 *p = static_cast<double2 *>(out) + blk_base<36>(s) + blk * 18 * SB;
   p[0] = make_double2(M[0].re, M[7].re);
-  p[(size_t)Vh] = make_double2(M[14].re, M[21].re);
-  p[(size_t)2 * Vh] = make_double2(M[28].re, M[35].re);
+  p[SB] = make_double2(M[14].re, M[21].re);
+  p[2 * SB] = make_double2(M[28].re, M[35].re);
   int k = 3;
   for (int i = 1; i < 6; i++)
-    for (int j = 0; j < i; j++, k++) p[(size_t)k * Vh] = make_double2(M[i * 6 + j].re, M[i * 6 + j].im);
+    for (int j = 0; j < i; j++, k++) p[k * SB] = make_double2(M[i * 6 + j].re, M[i * 6 + j].im);
 }
 
 // Hermitian inverse of a 6x6 block by LDL^H; returns false on a zero pivot
@@ -207,25 +207,28 @@ __global__ void k_clover_build(Geom g, GaugeView<GAOS64> U, int par, double coef
   for (int b = 0; b < 2; b++) {
     for (int k = 0; k < 36; k++) blk[b][k] = blk[b][k] * (-0.125 * coeff);
     for (int k = 0; k < 6; k++) blk[b][k * 7] += C(1.0, 0.0);
-    if (A64) block_store(A64, g.Vh, b, s, blk[b]);
+    if (A64) block_store(A64, b, s, blk[b]);
     if (Ainv64) {
       C inv[36];
       if (!herm6_inverse(blk[b], inv)) {
         atomicAdd(bad, 1);
         for (int k = 0; k < 36; k++) inv[k] = C(0, 0);
       }
-      block_store(Ainv64, g.Vh, b, s, inv);
+      block_store(Ainv64, b, s, inv);
     }
   }
 }
 
 __global__ void k_clover_to32(int Vh, const double2 *in, float4 *out) {
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < Vh; s += gridDim.x * blockDim.x)
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < Vh; s += gridDim.x * blockDim.x) {
+    const double2 *pi = in + blk_base<36>(s);
+    float4 *po = out + blk_base<18>(s);
     for (int b = 0; b < 2; b++)
       for (int k = 0; k < 9; k++) {
-        const double2 u = in[((size_t)b * 18 + 2 * k) * Vh + s], w = in[((size_t)b * 18 + 2 * k + 1) * Vh + s];
-        out[((size_t)b * 9 + k) * Vh + s] = make_float4((float)u.x, (float)u.y, (float)w.x, (float)w.y);
+        const double2 u = pi[(b * 18 + 2 * k) * SB], w = pi[(b * 18 + 2 * k + 1) * SB];
+        po[(b * 9 + k) * SB] = make_float4((float)u.x, (float)u.y, (float)w.x, (float)w.y);
       }
+  }
 }
 
 template <int K>
@@ -238,7 +241,7 @@ __global__ void k_clover_apply(int Vh, CloverView<CSOA64> cv, const void *in, vo
   }
 }
 
-size_t clover_bytes(int ckind, int Vh) { return (size_t)2 * (ckind == CSOA64 ? 18 * 16 : 9 * 16) * Vh; }
+size_t clover_bytes(int ckind, int Vh) { return (size_t)2 * (ckind == CSOA64 ? 18 * 16 : 9 * 16) * pad_sites(Vh); }
 
 void launch_clover_build(const Geom &g, const void *gauge_pyq, int par, double coeff, void *A64, void *Ainv64, int *bad,
                          cudaStream_t s) {

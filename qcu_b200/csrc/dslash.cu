@@ -14,8 +14,13 @@
 
 namespace qcu {
 
+// resident blocks per SM requested from the register allocator: the FP64
+// kernels would otherwise take ~176 registers (2 blocks of 128 threads per SM);
+// 3 blocks fit in 170 registers without spills
+#define DSLASH_MIN_BLOCKS(K) (((K) == AOS64 || (K) == SOA64) ? 3 : 1)
+
 template <int K, int G, int C, bool CLOV, int NX, int RED>
-__global__ void __launch_bounds__(DSLASH_BLOCK) k_dslash(Geom g, DslashArgs a, RedCtx rc) {
+__global__ void __launch_bounds__(DSLASH_BLOCK, DSLASH_MIN_BLOCKS(K)) k_dslash(Geom g, DslashArgs a, RedCtx rc) {
   using T = typename SpinorReal<K>::T;
   if (!gate_open(rc.st, a.gate)) return;
   constexpr int NV = RED == RED_NONE ? 1 : (RED == RED_TS_TT ? 3 : (RED == RED_DOT_RT ? 2 : 1));
@@ -26,7 +31,7 @@ __global__ void __launch_bounds__(DSLASH_BLOCK) k_dslash(Geom g, DslashArgs a, R
   if (s < g.Vh) {
     Cpx<T> w[12];
     const SpinorView<K> in{const_cast<void *>(a.in), const_cast<float *>(a.in_norm), g.Vh};
-    const GaugeView<G> U{a.gauge, g.Vh};
+    const GaugeView<G> U{a.gauge, G == GAOS64 ? g.Vh : pad_sites(g.Vh)};
     wilson_hop_site<K, G, T>(w, in, U, g, s, a.parity, (T)a.t_bc);
     if constexpr (CLOV) clover_apply_site<C, T>(CloverView<C>{a.clover, g.Vh}, s, w);
     const T aa = (T)a.a;
@@ -117,6 +122,7 @@ void launch_dslash(int kind, int gkind, int ckind, const Geom &g, const DslashAr
   else if (kind == SOA64 && gkind == GSOA64 && ckind == CSOA64) launch_clov<SOA64, GSOA64, CSOA64>(g, a, ctx, s);
   else if (kind == SOA32 && gkind == GSOA32 && ckind == CSOA32) launch_clov<SOA32, GSOA32, CSOA32>(g, a, ctx, s);
   else if (kind == SOA16 && gkind == GSOA16 && ckind == CSOA32) launch_clov<SOA16, GSOA16, CSOA32>(g, a, ctx, s);
+  else if (kind == SOA32 && gkind == GSOA16 && ckind == CSOA32) launch_clov<SOA32, GSOA16, CSOA32>(g, a, ctx, s);
   else throw Error(1, "dslash: unsupported storage combination");
 }
 

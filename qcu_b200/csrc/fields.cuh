@@ -1,22 +1,29 @@
 // Device-side views of the lattice fields and the Wilson stencil core.
 //
-// Storage kinds (one parity, Vh sites, `stride` elements per component):
+// Internal fields use a site-blocked layout: sites are grouped in blocks of
+// SB = 32 (one warp), and within a block every 16-byte (8-byte for 16-bit
+// links) component is stored for the 32 sites contiguously:
+//     element (site s, component c) at ((s / 32) * NC + c) * 32 + s % 32
+// so a warp's load of one component is one contiguous 512 (256) byte
+// segment, and the components of a site sit at compile-time offsets from one
+// base pointer (no per-component address arithmetic).  Vh is padded to a
+// multiple of 32; padding sites are never read or written.
+// Spinor kinds (one parity):
 //   AOS64 : PyQuda's own layout, complex128 [site][spin*3+colour]
 //           (python/PyQuda/pyquda/field.py:78,230) -- used by the legacy ABI
 //           so a single dslash needs no layout conversion at all.
-//   SOA64 : double2 [12][stride]    component-major, one 16-byte load per
-//           component, 512 contiguous bytes per warp instruction.
-//   SOA32 : float4  [6][stride]     two complex components per 16-byte load.
-//   SOA16 : uint4   [3][stride] + float norm[stride]   16-bit fixed point
+//   SOA64 : double2, NC = 12 (one complex per 16-byte load)
+//   SOA32 : float4,  NC = 6  (two complex per 16-byte load)
+//   SOA16 : uint4,   NC = 3  + float norm[Vh]: 16-bit fixed point
 //           (int16, value/norm * 32767) scaled by the per-site max |component|,
 //           four complex per 16-byte load.  Fixed point keeps 15 bits of
 //           mantissa relative to the site maximum where FP16 keeps 11.
 // Gauge kinds (reconstruct-12: rows 0 and 1 stored, row 2 = conj(r0 x r1),
-// include/define.h:198-206):
+// include/define.h:198-206), one slab of Vh_pad sites per (dir, parity):
 //   GAOS64 : PyQuda layout complex128 [dir][par][site][3][3], rows 0-1 read
-//   GSOA64 : double2 [dir][par][6][stride]
-//   GSOA32 : float4  [dir][par][3][stride]
-//   GSOA16 : uint2   [dir][par][3][stride]   (four int16 fixed point per load, |U_ij| <= 1)
+//   GSOA64 : double2, NC = 6
+//   GSOA32 : float4,  NC = 3
+//   GSOA16 : uint2,   NC = 3   (four int16 fixed point per load, |U_ij| <= 1)
 #pragma once
 #include "cplx.cuh"
 
@@ -46,6 +53,14 @@ __device__ __forceinline__ float2 fix16_unpack(unsigned w) {
   return make_float2(lo, hi);
 }
 
+// site-blocked indexing
+constexpr int SB = 32;
+__host__ __device__ __forceinline__ int pad_sites(int Vh) { return (Vh + SB - 1) / SB * SB; }
+template <int NC>
+__host__ __device__ __forceinline__ size_t blk_base(int s) {
+  return (size_t)(s >> 5) * NC * SB + (s & (SB - 1));
+}
+
 // Lattice geometry of one parity (half lattice).  Site index
 // i = ((t*Lz + z)*Ly + y)*Lxh + xh, the PyQuda/qcu ordering.
 struct Geom {
@@ -72,26 +87,26 @@ __device__ __forceinline__ void spinor_load(const SpinorView<K> &v, int s, Cpx<T
       out[c] = Cpx<T>((T)d.x, (T)d.y);
     }
   } else if constexpr (K == SOA64) {
-    const double2 *p = static_cast<const double2 *>(v.p) + s;
+    const double2 *p = static_cast<const double2 *>(v.p) + blk_base<12>(s);
 #pragma unroll
     for (int c = 0; c < 12; c++) {
-      double2 d = __ldg(p + (size_t)c * v.stride);
+      double2 d = __ldg(p + c * SB);
       out[c] = Cpx<T>((T)d.x, (T)d.y);
     }
   } else if constexpr (K == SOA32) {
-    const float4 *p = static_cast<const float4 *>(v.p) + s;
+    const float4 *p = static_cast<const float4 *>(v.p) + blk_base<6>(s);
 #pragma unroll
     for (int c = 0; c < 6; c++) {
-      float4 d = __ldg(p + (size_t)c * v.stride);
+      float4 d = __ldg(p + c * SB);
       out[2 * c] = Cpx<T>((T)d.x, (T)d.y);
       out[2 * c + 1] = Cpx<T>((T)d.z, (T)d.w);
     }
   } else {
-    const uint4 *p = static_cast<const uint4 *>(v.p) + s;
+    const uint4 *p = static_cast<const uint4 *>(v.p) + blk_base<3>(s);
     const float nrm = __ldg(v.norm + s) * (1.0f / FIX16_SCALE);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      uint4 d = __ldg(p + (size_t)c * v.stride);
+      uint4 d = __ldg(p + c * SB);
       unsigned w[4] = {d.x, d.y, d.z, d.w};
 #pragma unroll
       for (int k = 0; k < 4; k++) {
@@ -102,6 +117,22 @@ __device__ __forceinline__ void spinor_load(const SpinorView<K> &v, int s, Cpx<T
   }
 }
 
+// SOA16 without the per-site scale: values in units of norm/32767, and the norm
+__device__ __forceinline__ float spinor16_load_raw(const SpinorView<SOA16> &v, int s, Cpx<float> out[12]) {
+  const uint4 *p = static_cast<const uint4 *>(v.p) + blk_base<3>(s);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    uint4 d = __ldg(p + c * SB);
+    unsigned w[4] = {d.x, d.y, d.z, d.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const float2 f = fix16_unpack(w[k]);
+      out[4 * c + k] = Cpx<float>(f.x, f.y);
+    }
+  }
+  return __ldg(v.norm + s);
+}
+
 template <int K, typename T>
 __device__ __forceinline__ void spinor_store(const SpinorView<K> &v, int s, const Cpx<T> in[12]) {
   if constexpr (K == AOS64) {
@@ -109,27 +140,26 @@ __device__ __forceinline__ void spinor_store(const SpinorView<K> &v, int s, cons
 #pragma unroll
     for (int c = 0; c < 12; c++) p[c] = make_double2((double)in[c].re, (double)in[c].im);
   } else if constexpr (K == SOA64) {
-    double2 *p = static_cast<double2 *>(v.p) + s;
+    double2 *p = static_cast<double2 *>(v.p) + blk_base<12>(s);
 #pragma unroll
-    for (int c = 0; c < 12; c++) p[(size_t)c * v.stride] = make_double2((double)in[c].re, (double)in[c].im);
+    for (int c = 0; c < 12; c++) p[c * SB] = make_double2((double)in[c].re, (double)in[c].im);
   } else if constexpr (K == SOA32) {
-    float4 *p = static_cast<float4 *>(v.p) + s;
+    float4 *p = static_cast<float4 *>(v.p) + blk_base<6>(s);
 #pragma unroll
     for (int c = 0; c < 6; c++)
-      p[(size_t)c * v.stride] = make_float4((float)in[2 * c].re, (float)in[2 * c].im, (float)in[2 * c + 1].re,
-                                            (float)in[2 * c + 1].im);
+      p[c * SB] = make_float4((float)in[2 * c].re, (float)in[2 * c].im, (float)in[2 * c + 1].re, (float)in[2 * c + 1].im);
   } else {
     float mx = 0.f;
 #pragma unroll
     for (int c = 0; c < 12; c++) mx = fmaxf(mx, fmaxf(fabsf((float)in[c].re), fabsf((float)in[c].im)));
     float inv = mx > 0.f ? 1.0f / mx : 0.f;
-    uint4 *p = static_cast<uint4 *>(v.p) + s;
+    uint4 *p = static_cast<uint4 *>(v.p) + blk_base<3>(s);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       unsigned w[4];
 #pragma unroll
       for (int k = 0; k < 4; k++) w[k] = fix16_pack((float)in[4 * c + k].re * inv, (float)in[4 * c + k].im * inv);
-      p[(size_t)c * v.stride] = make_uint4(w[0], w[1], w[2], w[3]);
+      p[c * SB] = make_uint4(w[0], w[1], w[2], w[3]);
     }
     v.norm[s] = mx;
   }
@@ -139,8 +169,14 @@ __device__ __forceinline__ void spinor_store(const SpinorView<K> &v, int s, cons
 template <int G>
 struct GaugeView {
   const void *p;
-  int stride;  // sites per (dir, parity) slab (= Vh)
+  int stride;  // sites per (dir, parity) slab: Vh for GAOS64, pad_sites(Vh) otherwise
 };
+
+__device__ __forceinline__ void su3_row2(Cpx<float> *m) {
+  m[6] = (m[1] * m[5] - m[2] * m[4]).conj();
+  m[7] = (m[2] * m[3] - m[0] * m[5]).conj();
+  m[8] = (m[0] * m[4] - m[1] * m[3]).conj();
+}
 
 // rows 0 and 1 of U_dir(site) on parity par, then row 2 = conj(row0 x row1)
 template <int G, typename T>
@@ -154,25 +190,25 @@ __device__ __forceinline__ void link_load(const GaugeView<G> &u, int dir, int pa
       m[k] = Cpx<T>((T)d.x, (T)d.y);
     }
   } else if constexpr (G == GSOA64) {
-    const double2 *p = static_cast<const double2 *>(u.p) + slab * 6 + s;
+    const double2 *p = static_cast<const double2 *>(u.p) + slab * 6 + blk_base<6>(s);
 #pragma unroll
     for (int k = 0; k < 6; k++) {
-      double2 d = __ldg(p + (size_t)k * u.stride);
+      double2 d = __ldg(p + k * SB);
       m[k] = Cpx<T>((T)d.x, (T)d.y);
     }
   } else if constexpr (G == GSOA32) {
-    const float4 *p = static_cast<const float4 *>(u.p) + slab * 3 + s;
+    const float4 *p = static_cast<const float4 *>(u.p) + slab * 3 + blk_base<3>(s);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      float4 d = __ldg(p + (size_t)k * u.stride);
+      float4 d = __ldg(p + k * SB);
       m[2 * k] = Cpx<T>((T)d.x, (T)d.y);
       m[2 * k + 1] = Cpx<T>((T)d.z, (T)d.w);
     }
   } else {
-    const uint2 *p = static_cast<const uint2 *>(u.p) + slab * 3 + s;
+    const uint2 *p = static_cast<const uint2 *>(u.p) + slab * 3 + blk_base<3>(s);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      uint2 d = __ldg(p + (size_t)k * u.stride);
+      uint2 d = __ldg(p + k * SB);
       unsigned w[2] = {d.x, d.y};
 #pragma unroll
       for (int q = 0; q < 2; q++) {
@@ -184,6 +220,23 @@ __device__ __forceinline__ void link_load(const GaugeView<G> &u, int dir, int pa
   m[6] = (m[1] * m[5] - m[2] * m[4]).conj();
   m[7] = (m[2] * m[3] - m[0] * m[5]).conj();
   m[8] = (m[0] * m[4] - m[1] * m[3]).conj();
+}
+
+// GSOA16 link in units of 1/32767 (rows 0-1 as stored; row 2 rebuilt and
+// brought to the same units by one factor 1/32767)
+__device__ __forceinline__ void link16_load_raw(const GaugeView<GSOA16> &u, int dir, int par, int s, Cpx<float> m[9]) {
+  const size_t slab = (size_t)(dir * 2 + par) * u.stride;
+  const uint2 *p = static_cast<const uint2 *>(u.p) + slab * 3 + blk_base<3>(s);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    uint2 d = __ldg(p + k * SB);
+    const float2 a = fix16_unpack(d.x), b = fix16_unpack(d.y);
+    m[2 * k] = Cpx<float>(a.x, a.y);
+    m[2 * k + 1] = Cpx<float>(b.x, b.y);
+  }
+  su3_row2(m);
+#pragma unroll
+  for (int k = 6; k < 9; k++) m[k] = m[k] * (1.0f / FIX16_SCALE);
 }
 
 // ------------------------------------------------------------------ stencil
@@ -200,11 +253,11 @@ __host__ __device__ constexpr int gim(int mu, int r) {
   return mu == 0 ? (r < 2 ? 1 : -1) : (mu == 2 ? ((r == 0 || r == 3) ? 1 : -1) : 0);
 }
 
-// acc += U (1 - gamma_mu) psi   (FWD)   or   acc += U^dag (1 + gamma_mu) psi   (!FWD)
-// The projector has rank 2: rows 0,1 give h_k = psi_k + sigma*g_k*psi_col(k);
-// rows 2,3 are sigma*g_m * h_col(m).
-template <int MU, bool FWD, typename T>
-__device__ __forceinline__ void hop(Cpx<T> acc[12], const Cpx<T> psi[12], const Cpx<T> u[9], T phase) {
+// acc += f U (1 - gamma_mu) psi   (FWD)   or   acc += f U^dag (1 + gamma_mu) psi   (!FWD)
+// (f applied only when SCALED).  The projector has rank 2: rows 0,1 give
+// h_k = psi_k + sigma*g_k*psi_col(k); rows 2,3 are sigma*g_m * h_col(m).
+template <int MU, bool FWD, bool SCALED, typename T>
+__device__ __forceinline__ void hop(Cpx<T> acc[12], const Cpx<T> psi[12], const Cpx<T> u[9], T f) {
   constexpr int S = FWD ? -1 : 1;
   Cpx<T> h[2][3], uh[2][3];
 #pragma unroll
@@ -226,7 +279,7 @@ __device__ __forceinline__ void hop(Cpx<T> acc[12], const Cpx<T> psi[12], const 
         s += cdotmul(u[1 * 3 + r], h[k][1]);
         s += cdotmul(u[2 * 3 + r], h[k][2]);
       }
-      if constexpr (MU == 3) s = s * phase;
+      if constexpr (SCALED) s = s * f;
       uh[k][r] = s;
     }
   }
@@ -236,6 +289,32 @@ __device__ __forceinline__ void hop(Cpx<T> acc[12], const Cpx<T> psi[12], const 
     acc[3 + c] += uh[1][c];
     acc[6 + c] += unit_mul<S * gre(MU, 2), S * gim(MU, 2)>(uh[gcol(MU, 2)][c]);
     acc[9 + c] += unit_mul<S * gre(MU, 3), S * gim(MU, 3)>(uh[gcol(MU, 3)][c]);
+  }
+}
+
+// One hop: neighbour spinor n, link U_MU on (lpar, ls), boundary phase ph.
+// The 16-bit path multiplies in integer units and applies the spinor norm,
+// both fixed-point scales and the phase once, to the projected product.
+template <int MU, bool FWD, int K, int G, typename T>
+__device__ __forceinline__ void hop_from(Cpx<T> acc[12], const SpinorView<K> &in, const GaugeView<G> &U, int n,
+                                         int lpar, int ls, T ph) {
+  if constexpr (K == SOA16 && G == GSOA16) {
+    static_assert(sizeof(T) == 4, "16-bit storage computes in FP32");
+    Cpx<float> psi[12], u[9];
+    const float nrm = spinor16_load_raw(in, n, psi);
+    link16_load_raw(U, MU, lpar, ls, u);
+    hop<MU, FWD, true, float>(acc, psi, u, nrm * (1.0f / (FIX16_SCALE * FIX16_SCALE)) * ph);
+  } else if constexpr (K == SOA32 && G == GSOA16) {
+    // FP32 spinors with 16-bit links: the link scale folds into the hop factor
+    Cpx<float> psi[12], u[9];
+    spinor_load<K, float>(in, n, psi);
+    link16_load_raw(U, MU, lpar, ls, u);
+    hop<MU, FWD, true, float>(acc, psi, u, (1.0f / FIX16_SCALE) * ph);
+  } else {
+    Cpx<T> psi[12], u[9];
+    spinor_load<K, T>(in, n, psi);
+    link_load<G, T>(U, MU, lpar, ls, u);
+    hop<MU, FWD, MU == 3, T>(acc, psi, u, ph);
   }
 }
 
@@ -254,66 +333,51 @@ __device__ __forceinline__ void wilson_hop_site(Cpx<T> acc[12], const SpinorView
   const int z = r % g.Lz;
   const int t = r / g.Lz;
   const int xodd = (y + z + t + par) & 1;  // full x = 2*xh + xodd
-  Cpx<T> psi[12], u[9];
   int n;
   // x
   n = xodd ? (xh == g.Lxh - 1 ? s - xh : s + 1) : s;
-  spinor_load<K, T>(in, n, psi);
-  link_load<G, T>(U, 0, par, s, u);
-  hop<0, true, T>(acc, psi, u, T(1));
+  hop_from<0, true>(acc, in, U, n, par, s, T(1));
   n = xodd ? s : (xh == 0 ? s + g.Lxh - 1 : s - 1);
-  spinor_load<K, T>(in, n, psi);
-  link_load<G, T>(U, 0, 1 - par, n, u);
-  hop<0, false, T>(acc, psi, u, T(1));
+  hop_from<0, false>(acc, in, U, n, 1 - par, n, T(1));
   // y
   n = (y == g.Ly - 1) ? s - (g.Ly - 1) * g.sy : s + g.sy;
-  spinor_load<K, T>(in, n, psi);
-  link_load<G, T>(U, 1, par, s, u);
-  hop<1, true, T>(acc, psi, u, T(1));
+  hop_from<1, true>(acc, in, U, n, par, s, T(1));
   n = (y == 0) ? s + (g.Ly - 1) * g.sy : s - g.sy;
-  spinor_load<K, T>(in, n, psi);
-  link_load<G, T>(U, 1, 1 - par, n, u);
-  hop<1, false, T>(acc, psi, u, T(1));
+  hop_from<1, false>(acc, in, U, n, 1 - par, n, T(1));
   // z
   n = (z == g.Lz - 1) ? s - (g.Lz - 1) * g.sz : s + g.sz;
-  spinor_load<K, T>(in, n, psi);
-  link_load<G, T>(U, 2, par, s, u);
-  hop<2, true, T>(acc, psi, u, T(1));
+  hop_from<2, true>(acc, in, U, n, par, s, T(1));
   n = (z == 0) ? s + (g.Lz - 1) * g.sz : s - g.sz;
-  spinor_load<K, T>(in, n, psi);
-  link_load<G, T>(U, 2, 1 - par, n, u);
-  hop<2, false, T>(acc, psi, u, T(1));
+  hop_from<2, false>(acc, in, U, n, 1 - par, n, T(1));
   // t
   n = (t == g.Lt - 1) ? s - (g.Lt - 1) * g.st : s + g.st;
-  spinor_load<K, T>(in, n, psi);
-  link_load<G, T>(U, 3, par, s, u);
-  hop<3, true, T>(acc, psi, u, (t == g.Lt - 1) ? t_bc : T(1));
+  hop_from<3, true>(acc, in, U, n, par, s, (t == g.Lt - 1) ? t_bc : T(1));
   n = (t == 0) ? s + (g.Lt - 1) * g.st : s - g.st;
-  spinor_load<K, T>(in, n, psi);
-  link_load<G, T>(U, 3, 1 - par, n, u);
-  hop<3, false, T>(acc, psi, u, (t == 0) ? t_bc : T(1));
+  hop_from<3, false>(acc, in, U, n, 1 - par, n, (t == 0) ? t_bc : T(1));
 }
 
 // ------------------------------------------------------------------ clover
 // Packed clover (or inverse clover) per site: two Hermitian 6x6 chiral blocks
 // (spins {0,1} and {2,3} in the DeGrand-Rossi basis), each 36 reals:
 //   d[0..5] real diagonal, then L[i][j] (i>j) complex at i(i-1)/2 + j.
-// CSOA64: double2 [2][18][stride]   (diag packed as 3 double2, then 15)
-// CSOA32: float4  [2][9][stride]
+// Site-blocked like the spinors:
+// CSOA64: double2, NC = 36 per site (block b at components 18b..18b+17:
+//         the diagonal packed in 3 double2, then the 15 complex entries)
+// CSOA32: float4,  NC = 18 per site (block b at components 9b..9b+8)
 enum CloverKind { CSOA64 = 0, CSOA32 = 1 };
 template <int C>
 struct CloverView {
   const void *p;
-  int stride;
+  int stride;  // unused by the site-blocked layout (kept for symmetry with GaugeView)
 };
 
 template <int C, typename T>
 __device__ __forceinline__ void clover_block_load(const CloverView<C> &cv, int blk, int s, T d[6], Cpx<T> L[15]) {
   if constexpr (C == CSOA64) {
-    const double2 *p = static_cast<const double2 *>(cv.p) + (size_t)blk * 18 * cv.stride + s;
+    const double2 *p = static_cast<const double2 *>(cv.p) + blk_base<36>(s) + blk * 18 * SB;
     double2 q[18];
 #pragma unroll
-    for (int k = 0; k < 18; k++) q[k] = __ldg(p + (size_t)k * cv.stride);
+    for (int k = 0; k < 18; k++) q[k] = __ldg(p + k * SB);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       d[2 * k] = (T)q[k].x;
@@ -322,11 +386,11 @@ __device__ __forceinline__ void clover_block_load(const CloverView<C> &cv, int b
 #pragma unroll
     for (int k = 0; k < 15; k++) L[k] = Cpx<T>((T)q[3 + k].x, (T)q[3 + k].y);
   } else {
-    const float4 *p = static_cast<const float4 *>(cv.p) + (size_t)blk * 9 * cv.stride + s;
+    const float4 *p = static_cast<const float4 *>(cv.p) + blk_base<18>(s) + blk * 9 * SB;
     float f[36];
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-      float4 q = __ldg(p + (size_t)k * cv.stride);
+      float4 q = __ldg(p + k * SB);
       f[4 * k] = q.x;
       f[4 * k + 1] = q.y;
       f[4 * k + 2] = q.z;

@@ -12,16 +12,19 @@ namespace qcu {
 
 using C = Cpx<double>;
 
-__device__ __forceinline__ void ld12(const double2 *p, int s, int Vh, C v[12]) {
+// site-blocked FP64 spinor access (fields.cuh)
+__device__ __forceinline__ void ld12(const double2 *p, int s, int, C v[12]) {
+  p += blk_base<12>(s);
 #pragma unroll
   for (int c = 0; c < 12; c++) {
-    const double2 d = __ldg(p + (size_t)c * Vh + s);
+    const double2 d = __ldg(p + c * SB);
     v[c] = C(d.x, d.y);
   }
 }
-__device__ __forceinline__ void st12(double2 *p, int s, int Vh, const C v[12]) {
+__device__ __forceinline__ void st12(double2 *p, int s, int, const C v[12]) {
+  p += blk_base<12>(s);
 #pragma unroll
-  for (int c = 0; c < 12; c++) p[(size_t)c * Vh + s] = make_double2(v[c].re, v[c].im);
+  for (int c = 0; c < 12; c++) p[c * SB] = make_double2(v[c].re, v[c].im);
 }
 
 // sums[2j], sums[2j+1] = <W_j, w>, j < k
@@ -35,10 +38,10 @@ __global__ void __launch_bounds__(BLAS_BLOCK) k_gcr_multidot(int Vh, GcrArgs a, 
 #pragma unroll
     for (int j = 0; j < GCR_MAXK; j++) {
       if (j < a.k) {
-        const double2 *Wj = static_cast<const double2 *>(a.W[j]);
+        const double2 *Wj = static_cast<const double2 *>(a.W[j]) + blk_base<12>(s);
 #pragma unroll
         for (int c = 0; c < 12; c++) {
-          const double2 q = __ldg(Wj + (size_t)c * Vh + s);
+          const double2 q = __ldg(Wj + c * SB);
           red[2 * j] += q.x * w[c].re + q.y * w[c].im;
           red[2 * j + 1] += q.x * w[c].im - q.y * w[c].re;
         }

@@ -149,10 +149,11 @@ __global__ void k_fermion_random(int64_t n, double2 *psi, int kind, uint64_t see
 
 __global__ void k_uniform_soa64(int Vh, double2 *out, uint64_t seed) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < Vh; s += gridDim.x * blockDim.x) {
+    double2 *o = out + blk_base<12>(s);
 #pragma unroll
     for (int c = 0; c < 12; c++) {
       const uint64_t k = (uint64_t)s * 12 + c;
-      out[(size_t)c * Vh + s] = make_double2(rng_uniform(seed, 2 * k), rng_uniform(seed, 2 * k + 1));
+      o[c * SB] = make_double2(rng_uniform(seed, 2 * k), rng_uniform(seed, 2 * k + 1));
     }
   }
 }
@@ -161,27 +162,28 @@ __global__ void k_uniform_soa64(int Vh, double2 *out, uint64_t seed) {
 template <int G>
 __global__ void k_gauge_pack(int Vh, const double2 *__restrict__ in, void *out) {
   const int64_t n = (int64_t)8 * Vh;
+  const int64_t Vp = pad_sites(Vh);
   for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < n; l += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t slab = l / Vh, s = l % Vh;
+    const int64_t slab = l / Vh;
+    const int s = (int)(l % Vh);
     double2 v[6];
 #pragma unroll
     for (int k = 0; k < 6; k++) v[k] = in[l * 9 + k];
     if constexpr (G == GSOA64) {
-      double2 *o = static_cast<double2 *>(out) + slab * 6 * Vh + s;
+      double2 *o = static_cast<double2 *>(out) + slab * 6 * Vp + blk_base<6>(s);
 #pragma unroll
-      for (int k = 0; k < 6; k++) o[(size_t)k * Vh] = v[k];
+      for (int k = 0; k < 6; k++) o[k * SB] = v[k];
     } else if constexpr (G == GSOA32) {
-      float4 *o = static_cast<float4 *>(out) + slab * 3 * Vh + s;
+      float4 *o = static_cast<float4 *>(out) + slab * 3 * Vp + blk_base<3>(s);
 #pragma unroll
       for (int k = 0; k < 3; k++)
-        o[(size_t)k * Vh] = make_float4((float)v[2 * k].x, (float)v[2 * k].y, (float)v[2 * k + 1].x,
-                                        (float)v[2 * k + 1].y);
+        o[k * SB] = make_float4((float)v[2 * k].x, (float)v[2 * k].y, (float)v[2 * k + 1].x, (float)v[2 * k + 1].y);
     } else {
-      uint2 *o = static_cast<uint2 *>(out) + slab * 3 * Vh + s;
+      uint2 *o = static_cast<uint2 *>(out) + slab * 3 * Vp + blk_base<3>(s);
 #pragma unroll
       for (int k = 0; k < 3; k++)
-        o[(size_t)k * Vh] = make_uint2(fix16_pack((float)v[2 * k].x, (float)v[2 * k].y),
-                                       fix16_pack((float)v[2 * k + 1].x, (float)v[2 * k + 1].y));
+        o[k * SB] = make_uint2(fix16_pack((float)v[2 * k].x, (float)v[2 * k].y),
+                               fix16_pack((float)v[2 * k + 1].x, (float)v[2 * k + 1].y));
     }
   }
 }
@@ -208,10 +210,11 @@ void launch_uniform_soa64(int Vh, void *out, uint64_t seed, cudaStream_t s) {
 }
 
 size_t gauge_bytes(int gkind, int Vh) {
+  const size_t Vp = pad_sites(Vh);
   switch (gkind) {
-    case GSOA64: return (size_t)8 * 6 * Vh * 16;
-    case GSOA32: return (size_t)8 * 3 * Vh * 16;
-    case GSOA16: return (size_t)8 * 3 * Vh * 8;
+    case GSOA64: return 8 * 6 * Vp * 16;
+    case GSOA32: return 8 * 3 * Vp * 16;
+    case GSOA16: return 8 * 3 * Vp * 8;
     default: return (size_t)8 * 9 * Vh * 16;
   }
 }

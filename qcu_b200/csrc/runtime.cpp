@@ -55,15 +55,16 @@ Geom make_geom(const int latt[4]) {
 }
 
 size_t spinor_bytes(int kind, int Vh) {
+  const size_t Vp = pad_sites(Vh);  // site-blocked kinds are padded to whole blocks of 32
   switch (kind) {
-    case AOS64:
-    case SOA64: return (size_t)Vh * 12 * 16;
-    case SOA32: return (size_t)Vh * 12 * 8;
-    case SOA16: return (size_t)Vh * 12 * 4;
+    case AOS64: return (size_t)Vh * 12 * 16;
+    case SOA64: return Vp * 12 * 16;
+    case SOA32: return Vp * 12 * 8;
+    case SOA16: return Vp * 12 * 4;
   }
   return 0;
 }
-size_t spinor_norm_bytes(int kind, int Vh) { return kind == SOA16 ? (size_t)Vh * 4 : 0; }
+size_t spinor_norm_bytes(int kind, int Vh) { return kind == SOA16 ? (size_t)pad_sites(Vh) * 4 : 0; }
 
 // ---------------------------------------------------------------- buffers
 DevBuf::~DevBuf() { release(); }

@@ -91,6 +91,7 @@ struct Dsl {
   const GaugeHandle &G;
   Context &ctx;
   int kind;
+  int gkind = -1;  // gauge storage; -1: the one matching the spinor kind
   // out = a * [Ainv_par] D in + b1 x1 + b2 x2 (+ fused reduction)
   void operator()(int par, const Spinor &in, Spinor &out, bool clover, double a, const Spinor *x1 = nullptr,
                   double b1 = 0, const Spinor *x2 = nullptr, double b2 = 0, int red = RED_NONE, int fin = FIN_STORE,
@@ -114,7 +115,8 @@ struct Dsl {
       d.rt = rt->data.p;
       d.rt_norm = rt->norm.as<float>();
     }
-    d.gauge = G.gauge(kind);
+    const int gk = gkind >= 0 ? gkind : gkind_of(kind);
+    d.gauge = gk == GSOA64 ? G.g64.p : (gk == GSOA32 ? G.g32.p : G.g16.p);
     d.clover = clover ? G.clover_inv(kind, par) : nullptr;
     d.parity = par;
     d.t_bc = G.t_bc;
@@ -122,7 +124,7 @@ struct Dsl {
     d.red = red;
     d.fin = fin;
     d.gate = gate;
-    launch_dslash(kind, gkind_of(kind), ckind_of(kind), G.g, d, ctx, ctx.stream);
+    launch_dslash(kind, gk, ckind_of(kind), G.g, d, ctx, ctx.stream);
   }
 };
 
@@ -411,6 +413,10 @@ SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParam
   Workspace &w = workspace();
   w.prepare(kind, Vh);
   Dsl dP{G, ctx, kind}, d64{G, ctx, SOA64};
+  if (prm.gauge_precision) {
+    require(prm.gauge_precision == 16 && kind == SOA32, "solve: gauge_precision 16 is available with precision 32");
+    dP.gkind = GSOA16;
+  }
   // reduction partials sized once, before any graph capture bakes the pointer in
   ctx.ensure_partials((size_t)std::max((Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK, MAX_REDUCE_BLOCKS));
   const size_t half = spinor_bytes(AOS64, Vh);

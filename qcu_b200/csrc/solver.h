@@ -40,6 +40,7 @@ struct SolveParams {
   int inner_iters = 16;     // GCR: iterations of the inner solve per step
   double inner_tol = 0.1;   // GCR: inner solve stops at |r| <= inner_tol |r_outer|
   int gcr_k = 8;            // GCR: directions kept before a restart (<= 16)
+  int gauge_precision = 0;  // 0: links stored like the spinors; 16 with precision 32: 16-bit links
 };
 
 struct SolveInfo {

@@ -210,7 +210,7 @@ def test_invert_maxiter_reports_status(q):
     assert np.isfinite(host(x)).all()
 
 
-@pytest.mark.parametrize("prec", [32, 16])
+@pytest.mark.parametrize("prec", [32, 16, 3216])
 @pytest.mark.parametrize("clover", [False, True])
 def test_invert_gcr_true_residual(q, prec, clover):
     """Flexible GCR (FP64) preconditioned by a low-precision inner BiCGSTAB."""
@@ -222,8 +222,9 @@ def test_invert_gcr_true_residual(q, prec, clover):
     A = [O.clover_build(U, latt, p, c) for p in (0, 1)] if clover else [None, None]
     with q.Gauge(dev(U), latt, t_boundary=-1.0, clover_coeff=c if clover else 0.0) as G:
         x = empty_like_dev(O.full_shape(latt))
-        info = G.invert(x, dev(b), kappa, tol=1e-10, maxiter=5000, precision=prec, clover=clover, solver="gcr",
-                        inner_iters=12, gcr_k=6)
+        info = G.invert(x, dev(b), kappa, tol=1e-10, maxiter=5000, precision=32 if prec == 3216 else prec,
+                        gauge_precision=16 if prec == 3216 else 0, clover=clover, solver="gcr", inner_iters=12,
+                        gcr_k=6)
     assert info["status"] == 1, info
     assert info["true_residual"] <= 1e-10
     r = b - O.mfull(host(x), U, latt, kappa, -1.0, True, A[0], A[1])
