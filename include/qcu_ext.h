@@ -23,6 +23,7 @@ extern "C" {
 #endif
 
 typedef struct qcuGauge_s *qcuGauge;
+typedef struct qcuNN_s *qcuNN;  /* learned preconditioner (see qcuNNCreate) */
 
 /* last error of the calling thread: returns its code, copies the message */
 int qcuGetLastError(char *msg, int len);
@@ -65,6 +66,9 @@ typedef struct {
   int gcr_k;             /* GCR: directions kept before a restart (<= 16) */
   int gauge_precision;   /* 0: links stored like the spinors; 16 (with precision 32): FP32
                             spinors and 16-bit links in the inner operator */
+  int precond;           /* GCR preconditioner: 0 inner BiCGSTAB; 1 the network `nn`;
+                            2 the network, then the inner BiCGSTAB on what it leaves */
+  qcuNN nn;
 } qcuInvertParam;
 
 typedef struct {
@@ -102,6 +106,29 @@ int qcuFermionRandom(void *psi, long long n_complex, int kind, unsigned long lon
  *  - all calls share the scratch: calls that overlap on the GPU race. */
 int dslashCloverQcuNoAlloc(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, int parity);
 int qcuNoAllocMaxSites(void);
+
+/* Learned preconditioner: a gauge-equivariant parallel-transport network
+ * approximating M_pc^{-1} on the odd sites.  Two layers, 4 -> 16 -> 4
+ * colour-vector channels (12 complex -> 48 -> 12 per site); each layer sums
+ * the identity and the 8 link transports of its input, each mixed by a
+ * complex channel matrix.  FP32 arithmetic, FP32 master weights with a bf16
+ * copy used for inference.  Weights are qcuNNNumParams() floats (complex
+ * pairs, layer 1 [9][16][4] then layer 2 [9][4][16]).  Starts as the identity
+ * plus noise of scale init_scale. */
+int qcuNNCreate(qcuNN *net, unsigned long long seed, double init_scale);
+int qcuNNFree(qcuNN net);
+int qcuNNNumParams(void);
+int qcuNNGetWeights(qcuNN net, float *w);
+int qcuNNSetWeights(qcuNN net, const float *w);
+/* out = N(in) on odd-parity half spinors (complex128 PyQuda layout) */
+int qcuNNApply(qcuNN net, qcuGauge h, void *out, const void *in);
+/* One training step on a batch of (residual r_i, error e_i) odd half spinors
+ * ([batch][Vh][4][3] complex128): loss = mean_i |N(r_i) - e_i|^2 / |e_i|^2,
+ * gradients by the hand-written backward kernels, then an Adam step with
+ * learning rate lr (lr = 0: gradient only).  grad (optional, host) receives
+ * dL/dW* as qcuNNNumParams() floats. */
+int qcuNNTrainStep(qcuNN net, qcuGauge h, const void *r, const void *e, int batch, double lr, double *loss,
+                   float *grad);
 
 /* number of kernels this library has launched in this process (graph
  * replays count every node) */

@@ -77,6 +77,8 @@ class QcuInvertParam(ctypes.Structure):
         ("inner_tol", ctypes.c_double),
         ("gcr_k", ctypes.c_int),
         ("gauge_precision", ctypes.c_int),
+        ("precond", ctypes.c_int),
+        ("nn", ctypes.c_void_p),
     ]
 
 
@@ -122,6 +124,14 @@ _lib.dslashCloverQcuNoAlloc.argtypes = [_vp, _vp, _vp, _P, ctypes.c_int]
 _lib.dslashCloverQcuNoAlloc.restype = ctypes.c_int
 _lib.qcuNoAllocMaxSites.restype = ctypes.c_int
 _lib.qcuKernelLaunches.restype = ctypes.c_longlong
+_lib.qcuNNCreate.argtypes = [ctypes.POINTER(_vp), ctypes.c_ulonglong, ctypes.c_double]
+_lib.qcuNNFree.argtypes = [_vp]
+_lib.qcuNNNumParams.restype = ctypes.c_int
+_lib.qcuNNGetWeights.argtypes = [_vp, ctypes.c_void_p]
+_lib.qcuNNSetWeights.argtypes = [_vp, ctypes.c_void_p]
+_lib.qcuNNApply.argtypes = [_vp, _vp, _vp, _vp]
+_lib.qcuNNTrainStep.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                ctypes.c_void_p]
 _lib.qcuBenchDslash.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_double)]
 
@@ -247,7 +257,7 @@ class Gauge:
     def invert(self, x, b, kappa: float, tol: float = 1e-10, maxiter: int = 10000, precision: int = 64,
                delta: float = 0.1, clover: bool = False, x0_mode: int = 0, x0_seed: int = 0, abs_tol: bool = False,
                chunk: int = 0, solver: str = "bicgstab", inner_iters: int = 16, inner_tol: float = 0.1,
-               gcr_k: int = 8, gauge_precision: int = 0) -> dict:
+               gcr_k: int = 8, gauge_precision: int = 0, precond: int = 0, nn: "Network" = None) -> dict:
         """Solve M x = b (full spinors).  solver="bicgstab": BiCGSTAB in
         `precision` with FP64 reliable updates; solver="gcr": FP64 flexible
         GCR(gcr_k) preconditioned by `inner_iters` BiCGSTAB iterations in
@@ -259,6 +269,8 @@ class Gauge:
         p.solver = {"bicgstab": 0, "gcr": 1}[solver]
         p.inner_iters, p.inner_tol, p.gcr_k = inner_iters, inner_tol, gcr_k
         p.gauge_precision = gauge_precision
+        p.precond = precond
+        p.nn = nn._h.value if nn is not None else None
         r = QcuInvertResult()
         _check(_lib.qcuInvert(self._h, _ptr(x), _ptr(b), ctypes.byref(p), ctypes.byref(r)))
         return r.as_dict()
@@ -268,6 +280,57 @@ class Gauge:
         _check(_lib.qcuBenchDslash(self._h, int(precision), int(gauge_precision), int(clover), int(iters),
                                    ctypes.byref(ms)))
         return ms.value
+
+
+class Network:
+    """Learned preconditioner (qcuNN): a gauge-equivariant parallel-transport
+    network approximating M_pc^{-1}; see include/qcu_ext.h."""
+
+    def __init__(self, seed: int = 0, init_scale: float = 0.01):
+        self._h = _vp()
+        _check(_lib.qcuNNCreate(ctypes.byref(self._h), int(seed), float(init_scale)))
+
+    @staticmethod
+    def num_params() -> int:
+        return int(_lib.qcuNNNumParams())
+
+    def get_weights(self):
+        import numpy as np
+
+        w = np.empty(self.num_params(), np.float32)
+        _check(_lib.qcuNNGetWeights(self._h, w.ctypes.data))
+        return w
+
+    def set_weights(self, w):
+        import numpy as np
+
+        w = np.ascontiguousarray(w, np.float32)
+        assert w.size == self.num_params()
+        _check(_lib.qcuNNSetWeights(self._h, w.ctypes.data))
+
+    def apply(self, gauge: "Gauge", out, inp):
+        _check(_lib.qcuNNApply(self._h, gauge._h, _ptr(out), _ptr(inp)))
+
+    def train_step(self, gauge: "Gauge", r, e, batch: int, lr: float, want_grad: bool = False):
+        """Returns (loss, grad or None); r, e: [batch][Vh][4][3] complex128 device buffers."""
+        import numpy as np
+
+        loss = ctypes.c_double(0)
+        g = np.empty(self.num_params(), np.float32) if want_grad else None
+        _check(_lib.qcuNNTrainStep(self._h, gauge._h, _ptr(r), _ptr(e), int(batch), float(lr), ctypes.byref(loss),
+                                   g.ctypes.data if g is not None else None))
+        return loss.value, g
+
+    def close(self):
+        if self._h:
+            _lib.qcuNNFree(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def gauge_random(gauge, latt, kind: int = 0, eps: float = 0.25, seed: int = 0):

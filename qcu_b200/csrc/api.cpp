@@ -2,6 +2,7 @@
 // catches internal exceptions and turns them into a recorded last error.
 #include <cstring>
 
+#include "nn.h"
 #include "solver.h"
 
 // the library is built with hidden visibility; only the C ABI is exported
@@ -20,6 +21,9 @@ using namespace qcu;
 
 struct qcuGauge_s {
   GaugeHandle *h;
+};
+struct qcuNN_s {
+  NNet *n;
 };
 
 #define QCU_API_BEGIN \
@@ -166,6 +170,8 @@ void qcuInvertParamDefault(qcuInvertParam *p) {
   p->inner_tol = d.inner_tol;
   p->gcr_k = d.gcr_k;
   p->gauge_precision = d.gauge_precision;
+  p->precond = d.precond;
+  p->nn = nullptr;
 }
 
 int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuInvertResult *r) {
@@ -187,6 +193,8 @@ int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuIn
   s.inner_tol = p->inner_tol;
   s.gcr_k = p->gcr_k;
   s.gauge_precision = p->gauge_precision;
+  s.precond = p->precond;
+  s.nn = p->nn ? p->nn->n : nullptr;
   require(s.tol > 0, "tol must be positive");
   require(s.delta >= 0 && s.delta < 1, "delta must be in [0, 1)");
   SolveInfo info = solve(*h->h, x, b, s);
@@ -233,6 +241,54 @@ int dslashCloverQcuNoAlloc(void *fermion_out, void *fermion_in, void *gauge, Qcu
 }
 
 int qcuNoAllocMaxSites(void) { return noalloc_max_vh(); }
+
+int qcuNNCreate(qcuNN *net, unsigned long long seed, double init_scale) {
+  QCU_API_BEGIN
+  require(net != nullptr, "null network pointer");
+  *net = new qcuNN_s{nn_create(seed, init_scale)};
+  QCU_API_END
+}
+
+int qcuNNFree(qcuNN net) {
+  QCU_API_BEGIN
+  if (net) {
+    nn_free(net->n);
+    delete net;
+  }
+  QCU_API_END
+}
+
+int qcuNNNumParams(void) { return nn_nparam(); }
+
+int qcuNNGetWeights(qcuNN net, float *w) {
+  QCU_API_BEGIN
+  require(net && w, "null argument");
+  nn_get(*net->n, w);
+  QCU_API_END
+}
+
+int qcuNNSetWeights(qcuNN net, const float *w) {
+  QCU_API_BEGIN
+  require(net && w, "null argument");
+  nn_set(*net->n, w);
+  QCU_API_END
+}
+
+int qcuNNApply(qcuNN net, qcuGauge h, void *out, const void *in) {
+  QCU_API_BEGIN
+  require(net && h && out && in, "null argument");
+  nn_apply_pyq(*net->n, *h->h, out, in);
+  QCU_API_END
+}
+
+int qcuNNTrainStep(qcuNN net, qcuGauge h, const void *r, const void *e, int batch, double lr, double *loss,
+                   float *grad) {
+  QCU_API_BEGIN
+  require(net && h && r && e && batch > 0, "bad arguments");
+  const double l = nn_train_step(*net->n, *h->h, r, e, batch, lr, grad);
+  if (loss) *loss = l;
+  QCU_API_END
+}
 
 long long qcuKernelLaunches(void) { return launch_count(); }
 

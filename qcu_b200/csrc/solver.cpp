@@ -13,6 +13,7 @@
 #include <cstring>
 
 #include "gcr.h"
+#include "nn.h"
 #include "solver.h"
 
 namespace qcu {
@@ -220,7 +221,7 @@ static cudaGraphExec_t capture_inner_solve(Dsl &dP, Workspace &w, const VecSet &
 
 namespace {
 struct GcrSpace {
-  Spinor W[GCR_MAXK], Z[GCR_MAXK], znew, wnew;
+  Spinor W[GCR_MAXK], Z[GCR_MAXK], znew, wnew, zin;
   void prepare(int m, int Vh) {
     for (int j = 0; j < m; j++) {
       W[j].alloc(SOA64, Vh);
@@ -228,6 +229,7 @@ struct GcrSpace {
     }
     znew.alloc(SOA64, Vh);
     wnew.alloc(SOA64, Vh);
+    zin.alloc(SOA64, Vh);
   }
 };
 GcrSpace &gcr_space() {
@@ -255,11 +257,20 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
   init.maxiter = prm.inner_iters;
   *ctx.st_host = init;
   QCU_CUDA(cudaMemcpyAsync(ctx.st, ctx.st_host, sizeof(SolverState), cudaMemcpyHostToDevice, st));
+  // preconditioner: 0 inner solve z = BiCGSTAB(r); 1 z = N(r) (network);
+  // 2 z = N(r) + BiCGSTAB(r - M_pc N(r)).  The inner solve reads `rin`.
+  const int pc = prm.precond;
+  require(pc >= 0 && pc <= 2, "solve: precond must be 0, 1 or 2");
+  require(pc == 0 || prm.nn != nullptr, "solve: the network preconditioner needs a network");
+  if (pc != 0) nn_prepare(*prm.nn, Vh);
+  VecSet vin = vs;
+  vin.r64 = pc == 2 ? w.aux.data.p : w.r64.data.p;
   long long nodes = 0;
-  cudaGraphExec_t inner = capture_inner_solve(dP, w, vs, kappa, clov, prm.inner_iters, gs.znew, nodes);
+  cudaGraphExec_t inner =
+      pc == 1 ? nullptr : capture_inner_solve(dP, w, vin, kappa, clov, prm.inner_iters, gs.zin, nodes);
   GcrArgs a;
   a.w = gs.wnew.data.p;
-  a.z = gs.znew.data.p;
+  a.z = pc == 0 ? gs.zin.data.p : gs.znew.data.p;
   for (int j = 0; j < m; j++) {
     a.W[j] = gs.W[j].data.p;
     a.Z[j] = gs.Z[j].data.p;
@@ -282,11 +293,20 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
         break;
       }
       for (int k = 0; k < m && rr > tol2 && info.iterations < prm.maxiter; k++) {
-        QCU_CUDA(cudaGraphLaunch(inner, st));
-        note_launch(nodes);
+        if (pc != 0) nn_apply_soa64(*prm.nn, dP.G, w.r64.data.p, gs.znew.data.p, st);
+        if (pc == 2) {  // what the network leaves: aux = r - M_pc N(r)
+          d64(0, gs.znew, w.tmp64, clov, 1.0);
+          d64(1, w.tmp64, w.aux, clov, k2, &w.r64, 1.0, &gs.znew, -1.0);
+        }
+        if (pc != 1) {
+          QCU_CUDA(cudaGraphLaunch(inner, st));
+          note_launch(nodes);
+        }
+        if (pc == 2) launch_axpby(SOA64, Vh, 1.0, gs.zin.data.p, nullptr, 1.0, gs.znew.data.p, nullptr, st);
+        Spinor &zk = pc == 0 ? gs.zin : gs.znew;
         // w = M_pc z
-        d64(0, gs.znew, w.tmp64, clov, 1.0);
-        d64(1, w.tmp64, gs.wnew, clov, -k2, &gs.znew, 1.0);
+        d64(0, zk, w.tmp64, clov, 1.0);
+        d64(1, w.tmp64, gs.wnew, clov, -k2, &zk, 1.0);
         a.k = k;
         if (k > 0) {
           launch_gcr_multidot(Vh, a, ctx, st);
@@ -296,9 +316,9 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
             a.beta[2 * j] = S.sums[2 * j] / nw[j];
             a.beta[2 * j + 1] = S.sums[2 * j + 1] / nw[j];
           }
-          info.iterations += S.iter;  // inner iterations of this step
+          info.iterations += pc == 1 ? 1 : S.iter;  // inner iterations of this step
         } else {
-          info.iterations += read_state(ctx).iter;
+          info.iterations += pc == 1 ? 1 : read_state(ctx).iter;
         }
         launch_gcr_orth(Vh, a, ctx, st);
         SolverState S = read_state(ctx);
@@ -319,10 +339,10 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
       if (rr < 0) break;
     }
   } catch (...) {
-    cudaGraphExecDestroy(inner);
+    if (inner) cudaGraphExecDestroy(inner);
     throw;
   }
-  cudaGraphExecDestroy(inner);
+  if (inner) cudaGraphExecDestroy(inner);
   if (info.status == ST_RUNNING && info.iterations >= prm.maxiter) info.status = ST_MAXITER;
 }
 

@@ -41,6 +41,8 @@ struct SolveParams {
   double inner_tol = 0.1;   // GCR: inner solve stops at |r| <= inner_tol |r_outer|
   int gcr_k = 8;            // GCR: directions kept before a restart (<= 16)
   int gauge_precision = 0;  // 0: links stored like the spinors; 16 with precision 32: 16-bit links
+  int precond = 0;          // GCR: 0 inner BiCGSTAB, 1 network, 2 network then inner BiCGSTAB
+  struct NNet *nn = nullptr;
 };
 
 struct SolveInfo {
