@@ -215,7 +215,27 @@ __global__ void __launch_bounds__(BLAS_BLOCK) k_dots(int Vh, void *a, float *an,
   grid_reduce<4, BLAS_BLOCK>(red, RedCtx{st, partials, FIN_STORE});
 }
 
+// Condition of a device-side WHILE loop over solver iterations (a CUDA graph
+// conditional node): continue while the solver is not done.  The guard
+// bounds the loop whatever happens to `done`: after `cap` passes it stops
+// and reports the solve as having hit its iteration limit.
+__global__ void k_loop_cond(SolverState *st, cudaGraphConditionalHandle h, unsigned cap) {
+  const unsigned n = ++st->loop_guard;
+  bool go = st->done == 0;
+  if (go && n >= cap) {
+    st->status = ST_MAXITER;
+    st->done = 1;
+    go = false;
+  }
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
 // ---------------------------------------------------------------- launchers
+void launch_loop_cond(SolverState *st, cudaGraphConditionalHandle h, unsigned cap, cudaStream_t s) {
+  k_loop_cond<<<1, 1, 0, s>>>(st, h, cap);
+  QCU_CHECK_LAUNCH();
+}
+
 #define QCU_DISPATCH_K(kind, F, ...)                   \
   switch (kind) {                                      \
     case SOA64: F<SOA64> __VA_ARGS__; break;           \

@@ -144,6 +144,8 @@ void launch_xrupdate(int kind, int Vh, const VecSet &vs, Context &ctx, int gate,
 void launch_xfold(int kind, int Vh, const VecSet &vs, SolverState *st, int gate, cudaStream_t s);
 void launch_rconv(int kind, int Vh, const VecSet &vs, Context &ctx, int gate, cudaStream_t s);
 void launch_init(int kind, int Vh, const VecSet &vs, Context &ctx, cudaStream_t s);
+// device-side loop condition for a graph WHILE node: continue while !st->done (at most cap passes)
+void launch_loop_cond(SolverState *st, cudaGraphConditionalHandle h, unsigned cap, cudaStream_t s);
 void launch_convert(int kin, int kout, int Vh, const void *in, const float *in_n, void *out, float *out_n,
                     cudaStream_t s);
 void launch_axpby(int kind, int Vh, double a, void *x, float *xn, double b, void *y, float *yn, cudaStream_t s);

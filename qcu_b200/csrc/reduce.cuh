@@ -27,6 +27,7 @@ struct SolverState {
   int iter, maxiter, done, update, status, nupdates;
   int inner_mode;  // 1: a preconditioner solve (no reliable updates, stops on inner_rel2)
   unsigned ticket;
+  unsigned loop_guard;  // body executions of a device-side WHILE loop since the last init
 };
 
 // gate modes: which kernels of a captured iteration actually run
@@ -140,6 +141,7 @@ __device__ inline void finalize(SolverState *st, int op, const double *s) {
       st->update = 0;
       st->iter = 0;
       st->nupdates = 0;
+      st->loop_guard = 0;
       if (st->inner_mode) st->tol2 = st->inner_rel2 * s[2];
       if (bad_number(s[2])) {
         st->status = ST_NAN;

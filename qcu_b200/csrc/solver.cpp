@@ -219,6 +219,71 @@ static cudaGraphExec_t capture_inner_solve(Dsl &dP, Workspace &w, const VecSet &
   return exec;
 }
 
+// The same inner solve as a graph with a conditional WHILE node: init, then
+// the iteration body repeated on the device until the solver state says done
+// (converged, breakdown, or inner_iters reached; a guard counter bounds the
+// loop in any case), then the conversion.  No empty launches after
+// convergence and no host involvement.  `iters_out` is not known at capture
+// time: the caller reads st->iter after each replay.
+static cudaGraphExec_t capture_inner_solve_while(Dsl &dP, Workspace &w, const VecSet &vs, double kappa, bool clov,
+                                                 int iters, Spinor &z_out) {
+  Context &ctx = dP.ctx;
+  const int Vh = dP.G.g.Vh, kind = dP.kind;
+  const double k2 = kappa * kappa;
+  cudaStream_t st = ctx.stream;
+  const auto mode = cudaStreamCaptureModeThreadLocal;
+  const long long before = launch_count();
+  cudaGraph_t g = nullptr;
+  QCU_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphExec_t exec = nullptr;
+  try {
+    QCU_CUDA(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, mode));
+    launch_init(kind, Vh, vs, ctx, st);
+    QCU_CUDA(cudaStreamEndCapture(st, &g));
+    cudaGraphNode_t init_node;
+    size_t n = 1;
+    QCU_CUDA(cudaGraphGetNodes(g, &init_node, &n));
+    require(n == 1, "inner solve graph: unexpected init capture");
+    cudaGraphConditionalHandle h;
+    QCU_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t loop;
+    QCU_CUDA(cudaGraphAddNode(&loop, g, &init_node, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    QCU_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, mode));
+    launch_pupdate(kind, Vh, vs, ctx.st, GATE_NOT_DONE, st);
+    dP(0, w.p, w.tmp, clov, 1.0, nullptr, 0, nullptr, 0, RED_NONE, FIN_STORE, nullptr, GATE_NOT_DONE);
+    dP(1, w.tmp, w.v, clov, -k2, &w.p, 1.0, nullptr, 0, RED_DOT_RT, FIN_ALPHA, &w.rt, GATE_NOT_DONE);
+    launch_supdate(kind, Vh, vs, ctx.st, GATE_NOT_DONE, st);
+    dP(0, w.s, w.tmp, clov, 1.0, nullptr, 0, nullptr, 0, RED_NONE, FIN_STORE, nullptr, GATE_NOT_DONE);
+    dP(1, w.tmp, w.t, clov, -k2, &w.s, 1.0, nullptr, 0, RED_TS_TT, FIN_OMEGA, nullptr, GATE_NOT_DONE);
+    launch_xrupdate(kind, Vh, vs, ctx, GATE_NOT_DONE, st);
+    launch_loop_cond(ctx.st, h, (unsigned)iters + 2u, st);
+    QCU_CUDA(cudaStreamEndCapture(st, &body));
+    QCU_CUDA(cudaStreamBeginCaptureToGraph(st, g, &loop, nullptr, 1, mode));
+    launch_convert(w.x.kind, SOA64, Vh, w.x.data.p, w.x.norm.as<float>(), z_out.data.p, nullptr, st);
+    QCU_CUDA(cudaStreamEndCapture(st, &g));
+    QCU_CUDA(cudaGraphInstantiate(&exec, g, 0));
+  } catch (...) {
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+      cudaGraph_t junk;
+      cudaStreamEndCapture(st, &junk);
+    }
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    set_launch_count(before);
+    throw;
+  }
+  cudaGraphDestroy(g);
+  set_launch_count(before);  // replays are counted from the iteration count
+  return exec;
+}
+
 namespace {
 struct GcrSpace {
   Spinor W[GCR_MAXK], Z[GCR_MAXK], znew, wnew, zin;
@@ -265,9 +330,16 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
   if (pc != 0) nn_prepare(*prm.nn, Vh);
   VecSet vin = vs;
   vin.r64 = pc == 2 ? w.aux.data.p : w.r64.data.p;
-  long long nodes = 0;
-  cudaGraphExec_t inner =
-      pc == 1 ? nullptr : capture_inner_solve(dP, w, vin, kappa, clov, prm.inner_iters, gs.zin, nodes);
+  long long nodes = 0;  // 0: device-side WHILE loop (launches counted from the iteration count)
+  cudaGraphExec_t inner = nullptr;
+  if (pc != 1) {
+    try {
+      inner = capture_inner_solve_while(dP, w, vin, kappa, clov, prm.inner_iters, gs.zin);
+    } catch (const Error &) {
+      // conditional graph nodes unavailable: fixed-length capture with gated iterations
+      inner = capture_inner_solve(dP, w, vin, kappa, clov, prm.inner_iters, gs.zin, nodes);
+    }
+  }
   GcrArgs a;
   a.w = gs.wnew.data.p;
   a.z = pc == 0 ? gs.zin.data.p : gs.znew.data.p;
@@ -300,7 +372,7 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
         }
         if (pc != 1) {
           QCU_CUDA(cudaGraphLaunch(inner, st));
-          note_launch(nodes);
+          if (nodes) note_launch(nodes);
         }
         if (pc == 2) launch_axpby(SOA64, Vh, 1.0, gs.zin.data.p, nullptr, 1.0, gs.znew.data.p, nullptr, st);
         Spinor &zk = pc == 0 ? gs.zin : gs.znew;
@@ -317,8 +389,11 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
             a.beta[2 * j + 1] = S.sums[2 * j + 1] / nw[j];
           }
           info.iterations += pc == 1 ? 1 : S.iter;  // inner iterations of this step
+          if (pc != 1 && !nodes) note_launch(2 + 8LL * std::max(S.iter, 1));
         } else {
-          info.iterations += pc == 1 ? 1 : read_state(ctx).iter;
+          const int it = pc == 1 ? 1 : read_state(ctx).iter;
+          info.iterations += it;
+          if (pc != 1 && !nodes) note_launch(2 + 8LL * std::max(it, 1));
         }
         launch_gcr_orth(Vh, a, ctx, st);
         SolverState S = read_state(ctx);

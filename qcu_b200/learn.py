@@ -21,8 +21,13 @@ import time
 import numpy as np
 
 
-def make_pairs(G, kappa: float, n_src: int, checkpoints, seed: int = 1, latt=None):
-    """Returns (r, e): complex64 tensors [n_src * len(checkpoints), Vh, 4, 3] on the GPU."""
+def make_pairs(G, kappa: float, n_src: int, checkpoints, seed: int = 1, n_random: int = -1):
+    """Returns (r, e): complex64 tensors [pairs, Vh, 4, 3] on the GPU.
+
+    Solver-iterate errors concentrate on the low modes; on their own they
+    teach the network to amplify, which hurts on the rough part of a
+    residual.  n_random pairs with white-noise errors (default: as many as
+    the solver pairs) make the loss also cover |N M - 1| on every mode."""
     import torch
 
     import qcu_b200 as q
@@ -42,9 +47,17 @@ def make_pairs(G, kappa: float, n_src: int, checkpoints, seed: int = 1, latt=Non
         for k in checkpoints:
             G.invert(xk, b, kappa, tol=1e-30, maxiter=int(k), precision=64, delta=0.0)
             e.copy_(xs[1] - xk[1])
+            if float(torch.linalg.vector_norm(e)) == 0.0:
+                continue  # the iterate is already the solution to the last bit
             G.matpc(r, e, kappa)
             rs.append(r.to(torch.complex64).clone())
             es.append(e.to(torch.complex64).clone())
+    n_random = len(rs) if n_random < 0 else n_random
+    for i in range(n_random):
+        q.fermion_random(e, e.numel(), 0, seed + 100000 + i)
+        G.matpc(r, e, kappa)
+        rs.append(r.to(torch.complex64).clone())
+        es.append(e.to(torch.complex64).clone())
     return torch.stack(rs), torch.stack(es)
 
 
