@@ -50,10 +50,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", type=int, default=16, choices=[16, 32, 64], help="inner precision of the chosen solver")
+    ap.add_argument("--precision", type=int, default=32, choices=[16, 32, 64], help="inner precision of the chosen solver")
     ap.add_argument("--solver", default="gcr", choices=["gcr", "bicgstab"], help="chosen solver")
-    ap.add_argument("--gauge-precision", type=int, default=0, choices=[0, 16], help="16: FP32 spinors with 16-bit links")
-    ap.add_argument("--inner-iters", type=int, default=64)
+    ap.add_argument("--gauge-precision", type=int, default=16, choices=[0, 16], help="16: FP32 spinors with 16-bit links")
+    ap.add_argument("--inner-iters", type=int, default=96)
     ap.add_argument("--inner-tol", type=float, default=0.05)
     ap.add_argument("--gcr-k", type=int, default=4)
     ap.add_argument("--kappa", type=float, default=KAPPA)
