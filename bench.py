@@ -7,10 +7,13 @@ Workload (one "step" = one full solve):
     U = exp(i eps H), eps = 0.25, reunitarised (seeded, generated on the GPU
     by the library's own generator);
   * source: complex normal N(0,1) per component (seeded);
-  * kappa chosen so the plain FP64 BiCGSTAB needs about 1000 iterations;
+  * kappa = 0.1303, as close to the critical point as the plain FP64
+    BiCGSTAB still converges on this field (620 iterations; at 0.1304 it
+    does not converge within 4000);
   * stop at a true relative residual ||b - M x|| / ||b|| <= 1e-10, recomputed
     in FP64 on the full two-parity system at the end of every solve.
-Timed: the chosen solver (mixed precision with FP64 reliable updates).  The
+Timed: the chosen solver (FP64 flexible GCR around an FP32-spinor /
+16-bit-link inner BiCGSTAB run as a CUDA graph with a device-side loop).  The
 plain FP64 BiCGSTAB on the same GPU, the dslash bandwidth and a CPU baseline
 (the FP64 CPU oracle, all host cores, bounded sample) are reported beside it.
 
@@ -36,12 +39,16 @@ T_BC = -1.0
 GAUGE_SEED = 20251203
 SRC_SEED = 7
 KAPPA = 0.1303            # plain FP64 BiCGSTAB: 620 iterations on this ensemble (0.1304: no convergence in 4000)
-PLAIN_ITERS_REF = 1000    # iteration count used to extrapolate the CPU sample when no GPU run is available
+PLAIN_ITERS_REF = 620     # plain FP64 iterations of this system (measured), used to extrapolate CPU samples
 TOL = 1e-10
 METRIC = "solve s to 1e-10 true residual, chosen vs plain FP64, 1 B200; dslash HBM GB/s"
 # algorithmic bytes per output site of the hopping term (in-spinor + 8 recon-12 links + out-spinor)
 DSLASH_BYTES = {"64": 192 + 8 * 96 + 192, "32": 96 + 8 * 48 + 96, "16": 52 + 8 * 24 + 52, "32/16": 96 + 8 * 24 + 96}
 DSLASH_FLOPS = 1320
+# DRAM bytes (read + write) per launch of each dslash storage at 32^3 x 64 from
+# one ncu capture each (profiles/k_dslash_*_32x32x32x64.txt)
+DSLASH_TRAFFIC = {"32/16": {"bytes": 387_750_000, "profile": "profiles/k_dslash_soa32_gsoa16_32x32x32x64.txt"},
+                  "64": {"bytes": 1_208_100_000, "profile": "profiles/k_dslash_soa64_32x32x32x64.txt"}}
 
 
 def parse():
@@ -275,8 +282,12 @@ def run_ours(args, world, rank, local, pg):
     key = f"{args.precision}/16" if args.gauge_precision == 16 else str(args.precision)
     dom = dsl[key]
     kname = {"64": "SOA64,GSOA64", "32": "SOA32,GSOA32", "16": "SOA16,GSOA16", "32/16": "SOA32,GSOA16"}[key]
+    tr = DSLASH_TRAFFIC.get(key) if latt == LATT else None
     roofline = {"bound": "hbm", "achieved": round(dom["GBps"], 1), "peak": pk, "unit": "GB/s",
-                "frac": round(dom["GBps"] / pk, 4), "traffic": None,
+                "frac": round(dom["GBps"] / pk, 4), "traffic": tr["bytes"] if tr else None,
+                "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
+                "traffic_source": tr["profile"] if tr else None,
+                "algorithmic_bytes": DSLASH_BYTES[key] * vh,
                 "kernel": f"k_dslash<{kname}> ({DSLASH_BYTES[key]} B/site x {vh} sites per launch)",
                 "peak_kind": pk_kind}
 

@@ -85,6 +85,40 @@ void qcuInvertParamDefault(qcuInvertParam *p);
 /* x, b: full spinors.  Even-odd preconditioned BiCGSTAB on the odd sites. */
 int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuInvertResult *r);
 
+/* One system of a batched solve: nrhs right-hand sides on one gauge handle.
+ * x and b hold nrhs full spinors back to back ([nrhs][2][Vh][4][3]
+ * complex128, PyQuda layout, device). */
+typedef struct {
+  qcuGauge gauge;
+  int nrhs;
+  double kappa;
+  int use_clover;
+  void *x;
+  const void *b;
+} qcuBatchSystem;
+
+/* Tunables the batched solver chose for this batch shape (autotuned on the
+ * first solve of a shape, reused afterwards). */
+typedef struct {
+  int dslash_threads;  /* sites per block of the inner dslash (64, 128, 256) */
+  int dslash_rhs;      /* right-hand sides each dslash thread computes (1, 2, 4) */
+  int blas_sites;      /* sites per block of the vector kernels */
+  int mma;             /* 1: the inner dslash uses the tensor-core contraction */
+} qcuBatchTune;
+
+/* Batched solve of every right-hand side of every system (at most 64 in
+ * total; lattices may differ in size): flexible GCR(gcr_k) in FP64 per
+ * right-hand side around one inner BiCGSTAB (precision 32 -- with 16-bit
+ * links when gauge_precision is 16 -- or 64) that advances all right-hand
+ * sides together, one kernel launch per step for the whole batch, captured
+ * as one CUDA graph.  Uses kappa/use_clover of each system (the param's are
+ * ignored), tol, maxiter (inner iterations per rhs), precision,
+ * gauge_precision, inner_iters, inner_tol and gcr_k; x0_mode must be 0 and
+ * abs_tol 0.  results: one per right-hand side, in system order (may be
+ * null); tune: optional. */
+int qcuInvertBatch(const qcuBatchSystem *systems, int n_systems, const qcuInvertParam *p, qcuInvertResult *results,
+                   qcuBatchTune *tune);
+
 /* seeded generators, PyQuda layout complex128 on the device.
  * gauge kind: 0 Haar SU(3), 1 exp(i eps H) reunitarised, 2 unit links.
  * fermion kind: 0 complex normal N(0,1) per component, 1 uniform (0,1]. */

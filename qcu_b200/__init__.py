@@ -97,6 +97,25 @@ class QcuInvertResult(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class QcuBatchSystem(ctypes.Structure):
+    _fields_ = [
+        ("gauge", ctypes.c_void_p),
+        ("nrhs", ctypes.c_int),
+        ("kappa", ctypes.c_double),
+        ("use_clover", ctypes.c_int),
+        ("x", ctypes.c_void_p),
+        ("b", ctypes.c_void_p),
+    ]
+
+
+class QcuBatchTune(ctypes.Structure):
+    _fields_ = [("dslash_threads", ctypes.c_int), ("dslash_rhs", ctypes.c_int), ("blas_sites", ctypes.c_int),
+                ("mma", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _P = ctypes.POINTER(QcuParam)
 for _name in ("dslashQcu", "dslashCloverQcu"):
     getattr(_lib, _name).argtypes = [_vp, _vp, _vp, _P, ctypes.c_int]
@@ -117,6 +136,8 @@ _lib.qcuMat.argtypes = [_vp, _vp, _vp, ctypes.c_double, ctypes.c_int]
 _lib.qcuInvertParamDefault.argtypes = [ctypes.POINTER(QcuInvertParam)]
 _lib.qcuInvertParamDefault.restype = None
 _lib.qcuInvert.argtypes = [_vp, _vp, _vp, ctypes.POINTER(QcuInvertParam), ctypes.POINTER(QcuInvertResult)]
+_lib.qcuInvertBatch.argtypes = [ctypes.POINTER(QcuBatchSystem), ctypes.c_int, ctypes.POINTER(QcuInvertParam),
+                                ctypes.POINTER(QcuInvertResult), ctypes.POINTER(QcuBatchTune)]
 _lib.qcuGaugeRandom.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong]
 _lib.qcuFermionRandom.argtypes = [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_ulonglong]
 _lib.qcuGetStream.restype = _vp
@@ -280,6 +301,71 @@ class Gauge:
         _check(_lib.qcuBenchDslash(self._h, int(precision), int(gauge_precision), int(clover), int(iters),
                                    ctypes.byref(ms)))
         return ms.value
+
+
+def invert_batch(systems, tol: float = 1e-10, maxiter: int = 10000, precision: int = 32, gauge_precision: int = 16,
+                 inner_iters: int = 96, inner_tol: float = 0.05, gcr_k: int = 4):
+    """Solve every right-hand side of every system together (qcuInvertBatch).
+
+    systems: sequence of (gauge, x, b, kappa, clover) with `gauge` a Gauge and
+    x, b contiguous complex128 CUDA tensors of nrhs full spinors
+    ([nrhs, 2, Lt, Lz, Ly, Lx/2, 4, 3]).  Lattices may differ between
+    systems.  Returns (one result dict per right-hand side in system order,
+    the tunables the autotuner chose)."""
+    sys_arr = (QcuBatchSystem * len(systems))()
+    nrhs_total = 0
+    for i, (G, x, b, kappa, clover) in enumerate(systems):
+        L = Layout(tuple(G.latt))
+        n = x.numel() // (2 * L.vh * 12)
+        if n * 2 * L.vh * 12 != x.numel() or b.numel() != x.numel():
+            raise ValueError("x and b must hold whole full spinors of the same count")
+        sys_arr[i].gauge = G._h.value
+        sys_arr[i].nrhs = n
+        sys_arr[i].kappa = float(kappa)
+        sys_arr[i].use_clover = int(bool(clover))
+        sys_arr[i].x = _ptr(x)
+        sys_arr[i].b = _ptr(b)
+        nrhs_total += n
+    p = QcuInvertParam()
+    _lib.qcuInvertParamDefault(ctypes.byref(p))
+    p.tol, p.maxiter, p.precision, p.gauge_precision = tol, maxiter, precision, gauge_precision
+    p.solver, p.inner_iters, p.inner_tol, p.gcr_k = 1, inner_iters, inner_tol, gcr_k
+    res = (QcuInvertResult * max(nrhs_total, 1))()
+    tune = QcuBatchTune()
+    _check(_lib.qcuInvertBatch(sys_arr, len(systems), ctypes.byref(p), res, ctypes.byref(tune)))
+    return [res[i].as_dict() for i in range(nrhs_total)], tune.as_dict()
+
+
+def point_sources(latt, origin, device="cuda"):
+    """The 12 point sources (source spin s, colour c at `origin` = [x, y, z, t])
+    of a propagator, PyQuda layout, [12 = s*3+c, 2, Lt, Lz, Ly, Lx/2, 4, 3]
+    (python/PyQuda/pyquda/utils/source.py:7-22)."""
+    import torch
+
+    L = Layout(tuple(latt))
+    x, y, z, t = [int(v) for v in origin]
+    b = torch.zeros((12,) + L.full, dtype=torch.complex128, device=device)
+    eo = (x + y + z + t) % 2
+    for s in range(4):
+        for c in range(3):
+            b[s * 3 + c, eo, t, z, y, x // 2, s, c] = 1.0
+    return b
+
+
+def invert12(G: "Gauge", kappa: float, origin, clover: bool = False, **kw):
+    """Propagator from a point source at `origin`: the 12 spin-colour solves in
+    one batched solve.  Returns (propagator [2, Lt, Lz, Ly, Lx/2, 4, 4, 3, 3] =
+    [.., sink spin, source spin, sink colour, source colour] -- PyQuda's
+    LatticePropagator layout, python/PyQuda/pyquda/core.py:44-57 --, the
+    per-source result dicts, the tunables)."""
+    import torch
+
+    b = point_sources(G.latt, origin, device="cuda")
+    x = torch.empty_like(b)
+    res, tune = invert_batch([(G, x, b, kappa, clover)], **kw)
+    L = Layout(tuple(G.latt))
+    prop = x.view((4, 3) + L.full).permute(2, 3, 4, 5, 6, 7, 0, 8, 1).contiguous()
+    return prop, res, tune
 
 
 class Network:

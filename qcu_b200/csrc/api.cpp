@@ -2,6 +2,7 @@
 // catches internal exceptions and turns them into a recorded last error.
 #include <cstring>
 
+#include "batch.h"
 #include "nn.h"
 #include "solver.h"
 
@@ -174,9 +175,7 @@ void qcuInvertParamDefault(qcuInvertParam *p) {
   p->nn = nullptr;
 }
 
-int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuInvertResult *r) {
-  QCU_API_BEGIN
-  require(h != nullptr && p != nullptr, "null handle or parameter pointer");
+static SolveParams solve_params(const qcuInvertParam *p) {
   SolveParams s;
   s.kappa = p->kappa;
   s.tol = p->tol;
@@ -197,15 +196,50 @@ int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuIn
   s.nn = p->nn ? p->nn->n : nullptr;
   require(s.tol > 0, "tol must be positive");
   require(s.delta >= 0 && s.delta < 1, "delta must be in [0, 1)");
-  SolveInfo info = solve(*h->h, x, b, s);
-  if (r) {
-    r->iterations = info.iterations;
-    r->reliable_updates = info.updates;
-    r->status = info.status;
-    r->restarts = info.restarts;
-    r->true_residual = info.true_residual;
-    r->iter_residual2 = info.iter_residual2;
-    r->seconds = info.seconds;
+  return s;
+}
+
+static void fill_result(const SolveInfo &info, qcuInvertResult *r) {
+  r->iterations = info.iterations;
+  r->reliable_updates = info.updates;
+  r->status = info.status;
+  r->restarts = info.restarts;
+  r->true_residual = info.true_residual;
+  r->iter_residual2 = info.iter_residual2;
+  r->seconds = info.seconds;
+}
+
+int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuInvertResult *r) {
+  QCU_API_BEGIN
+  require(h != nullptr && p != nullptr, "null handle or parameter pointer");
+  const SolveInfo info = solve(*h->h, x, b, solve_params(p));
+  if (r) fill_result(info, r);
+  QCU_API_END
+}
+
+int qcuInvertBatch(const qcuBatchSystem *systems, int n_systems, const qcuInvertParam *p, qcuInvertResult *results,
+                   qcuBatchTune *tune) {
+  QCU_API_BEGIN
+  require(systems != nullptr && p != nullptr && n_systems > 0, "null systems/parameter pointer or no systems");
+  std::vector<BatchSystem> sys(n_systems);
+  for (int i = 0; i < n_systems; i++) {
+    require(systems[i].gauge != nullptr, "batch: null gauge handle");
+    sys[i].G = systems[i].gauge->h;
+    sys[i].nrhs = systems[i].nrhs;
+    sys[i].kappa = systems[i].kappa;
+    sys[i].use_clover = systems[i].use_clover;
+    sys[i].x = systems[i].x;
+    sys[i].b = systems[i].b;
+  }
+  BatchTune t;
+  const std::vector<SolveInfo> info = solve_batch(sys, solve_params(p), &t);
+  if (results)
+    for (size_t r = 0; r < info.size(); r++) fill_result(info[r], results + r);
+  if (tune) {
+    tune->dslash_threads = t.dslash_threads;
+    tune->dslash_rhs = t.dslash_rhs;
+    tune->blas_sites = t.blas_sites;
+    tune->mma = t.mma;
   }
   QCU_API_END
 }

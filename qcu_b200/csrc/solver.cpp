@@ -18,7 +18,7 @@
 
 namespace qcu {
 
-static int kind_of_precision(int prec) {
+int kind_of_precision(int prec) {
   switch (prec) {
     case 64: return SOA64;
     case 32: return SOA32;
@@ -88,46 +88,38 @@ Workspace &workspace() {
 }
 }  // namespace
 
-struct Dsl {
-  const GaugeHandle &G;
-  Context &ctx;
-  int kind;
-  int gkind = -1;  // gauge storage; -1: the one matching the spinor kind
-  // out = a * [Ainv_par] D in + b1 x1 + b2 x2 (+ fused reduction)
-  void operator()(int par, const Spinor &in, Spinor &out, bool clover, double a, const Spinor *x1 = nullptr,
-                  double b1 = 0, const Spinor *x2 = nullptr, double b2 = 0, int red = RED_NONE, int fin = FIN_STORE,
-                  const Spinor *rt = nullptr, int gate = GATE_ALWAYS) {
-    DslashArgs d;
-    d.in = in.data.p;
-    d.in_norm = in.norm.as<float>();
-    d.out = out.data.p;
-    d.out_norm = out.norm.as<float>();
-    if (x1) {
-      d.x1 = x1->data.p;
-      d.x1_norm = x1->norm.as<float>();
-      d.b1 = b1;
-    }
-    if (x2) {
-      d.x2 = x2->data.p;
-      d.x2_norm = x2->norm.as<float>();
-      d.b2 = b2;
-    }
-    if (rt) {
-      d.rt = rt->data.p;
-      d.rt_norm = rt->norm.as<float>();
-    }
-    const int gk = gkind >= 0 ? gkind : gkind_of(kind);
-    d.gauge = gk == GSOA64 ? G.g64.p : (gk == GSOA32 ? G.g32.p : G.g16.p);
-    d.clover = clover ? G.clover_inv(kind, par) : nullptr;
-    d.parity = par;
-    d.t_bc = G.t_bc;
-    d.a = a;
-    d.red = red;
-    d.fin = fin;
-    d.gate = gate;
-    launch_dslash(kind, gk, ckind_of(kind), G.g, d, ctx, ctx.stream);
+void Dsl::operator()(int par, const Spinor &in, Spinor &out, bool clover, double a, const Spinor *x1, double b1,
+                     const Spinor *x2, double b2, int red, int fin, const Spinor *rt, int gate) {
+  DslashArgs d;
+  d.in = in.data.p;
+  d.in_norm = in.norm.as<float>();
+  d.out = out.data.p;
+  d.out_norm = out.norm.as<float>();
+  if (x1) {
+    d.x1 = x1->data.p;
+    d.x1_norm = x1->norm.as<float>();
+    d.b1 = b1;
   }
-};
+  if (x2) {
+    d.x2 = x2->data.p;
+    d.x2_norm = x2->norm.as<float>();
+    d.b2 = b2;
+  }
+  if (rt) {
+    d.rt = rt->data.p;
+    d.rt_norm = rt->norm.as<float>();
+  }
+  const int gk = gkind >= 0 ? gkind : gkind_of(kind);
+  d.gauge = gk == GSOA64 ? G.g64.p : (gk == GSOA32 ? G.g32.p : G.g16.p);
+  d.clover = clover ? G.clover_inv(kind, par) : nullptr;
+  d.parity = par;
+  d.t_bc = G.t_bc;
+  d.a = a;
+  d.red = red;
+  d.fin = fin;
+  d.gate = gate;
+  launch_dslash(kind, gk, ckind_of(kind), G.g, d, ctx, ctx.stream);
+}
 
 static VecSet make_vecset(Workspace &w) {
   VecSet vs;
@@ -159,6 +151,56 @@ static SolverState read_state(Context &ctx) {
 static double dots_norm2(Context &ctx, int kind, int Vh, void *a, float *an) {
   launch_dots(kind, Vh, a, an, a, an, ctx, ctx.stream);
   return read_state(ctx).sums[2];
+}
+
+double prepare_source(Dsl &d64, const void *b_pyq, double kappa, bool clov, Spinor &be, Spinor &bo, Spinor &bp,
+                      Spinor &aux, Spinor &tmp64) {
+  Context &ctx = d64.ctx;
+  const GaugeHandle &G = d64.G;
+  const int Vh = G.g.Vh;
+  cudaStream_t st = ctx.stream;
+  const char *b = static_cast<const char *>(b_pyq);
+  launch_convert(AOS64, SOA64, Vh, b, nullptr, be.data.p, nullptr, st);
+  launch_convert(AOS64, SOA64, Vh, b + spinor_bytes(AOS64, Vh), nullptr, bo.data.p, nullptr, st);
+  if (clov) {
+    launch_clover_apply(SOA64, Vh, G.Ainv64[0].p, be.data.p, aux.data.p, st);
+    d64(1, aux, tmp64, false, kappa, &bo, 1.0);
+    launch_clover_apply(SOA64, Vh, G.Ainv64[1].p, tmp64.data.p, bp.data.p, st);
+  } else {
+    d64(1, be, bp, false, kappa, &bo, 1.0);
+  }
+  return dots_norm2(ctx, SOA64, Vh, be.data.p, nullptr) + dots_norm2(ctx, SOA64, Vh, bo.data.p, nullptr);
+}
+
+double finish_solution(Dsl &d64, double kappa, bool clov, Spinor &be, Spinor &bo, Spinor &xo, Spinor &xe,
+                       Spinor &aux, Spinor &tmp64, void *x_pyq) {
+  Context &ctx = d64.ctx;
+  const GaugeHandle &G = d64.G;
+  const int Vh = G.g.Vh;
+  cudaStream_t st = ctx.stream;
+  // x_e = A_e^-1 (b_e + kappa D_eo x_o)
+  d64(0, xo, tmp64, false, kappa, &be, 1.0);
+  if (clov) launch_clover_apply(SOA64, Vh, G.Ainv64[0].p, tmp64.data.p, xe.data.p, st);
+  else launch_convert(SOA64, SOA64, Vh, tmp64.data.p, nullptr, xe.data.p, nullptr, st);
+  // full-system FP64 true residual: r_p = b_p - A_p x_p + kappa D x_{1-p}
+  double rr = 0;
+  for (int p = 0; p < 2; p++) {
+    Spinor &xp_ = p ? xo : xe;
+    Spinor &bpar = p ? bo : be;
+    const Spinor *ax = &xp_;
+    if (clov) {
+      launch_clover_apply(SOA64, Vh, G.A64[p].p, xp_.data.p, aux.data.p, st);
+      ax = &aux;
+    }
+    d64(p, p ? xe : xo, tmp64, false, kappa, &bpar, 1.0, ax, -1.0, RED_NORM, FIN_STORE);
+    rr += read_state(ctx).sums[0];
+  }
+  if (x_pyq) {
+    char *x = static_cast<char *>(x_pyq);
+    launch_convert(SOA64, AOS64, Vh, xe.data.p, nullptr, x, nullptr, st);
+    launch_convert(SOA64, AOS64, Vh, xo.data.p, nullptr, x + spinor_bytes(AOS64, Vh), nullptr, st);
+  }
+  return rr;
 }
 
 // one BiCGSTAB iteration (plus the gated reliable-update sequence)
@@ -515,22 +557,11 @@ SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParam
   // reduction partials sized once, before any graph capture bakes the pointer in
   ctx.ensure_partials((size_t)std::max((Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK, MAX_REDUCE_BLOCKS));
   const size_t half = spinor_bytes(AOS64, Vh);
-  const char *bp = static_cast<const char *>(b_pyq);
   char *xp = static_cast<char *>(x_pyq);
   cudaStream_t st = ctx.stream;
   QCU_CUDA(cudaDeviceSynchronize());  // inputs written on any stream are complete
 
-  // b_e, b_o -> FP64 internal; b'_o = A_o^-1 (b_o + kappa D_oe A_e^-1 b_e)
-  launch_convert(AOS64, SOA64, Vh, bp, nullptr, w.be.data.p, nullptr, st);
-  launch_convert(AOS64, SOA64, Vh, bp + half, nullptr, w.bo.data.p, nullptr, st);
-  if (clov) {
-    launch_clover_apply(SOA64, Vh, G.Ainv64[0].p, w.be.data.p, w.aux.data.p, st);
-    d64(1, w.aux, w.tmp64, false, kappa, &w.bo, 1.0);
-    launch_clover_apply(SOA64, Vh, G.Ainv64[1].p, w.tmp64.data.p, w.bp.data.p, st);
-  } else {
-    d64(1, w.be, w.bp, false, kappa, &w.bo, 1.0);
-  }
-  const double bb = dots_norm2(ctx, SOA64, Vh, w.be.data.p, nullptr) + dots_norm2(ctx, SOA64, Vh, w.bo.data.p, nullptr);
+  const double bb = prepare_source(d64, b_pyq, kappa, clov, w.be, w.bo, w.bp, w.aux, w.tmp64);
   SolveInfo info;
   if (bb == 0.0) {
     QCU_CUDA(cudaMemsetAsync(x_pyq, 0, 2 * half, st));
@@ -563,23 +594,7 @@ SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParam
         continue;
       }
     }
-    // x_e = A_e^-1 (b_e + kappa D_eo x_o)
-    d64(0, w.x64, w.tmp64, false, kappa, &w.be, 1.0);
-    if (clov) launch_clover_apply(SOA64, Vh, G.Ainv64[0].p, w.tmp64.data.p, w.xe.data.p, st);
-    else launch_convert(SOA64, SOA64, Vh, w.tmp64.data.p, nullptr, w.xe.data.p, nullptr, st);
-    // full-system FP64 true residual: r_p = b_p - A_p x_p + kappa D x_{1-p}
-    double rr = 0;
-    for (int p = 0; p < 2; p++) {
-      Spinor &xp_ = p ? w.x64 : w.xe;
-      Spinor &bpar = p ? w.bo : w.be;
-      const Spinor *ax = &xp_;
-      if (clov) {
-        launch_clover_apply(SOA64, Vh, G.A64[p].p, xp_.data.p, w.aux.data.p, st);
-        ax = &w.aux;
-      }
-      d64(p, p ? w.xe : w.x64, w.tmp64, false, kappa, &bpar, 1.0, ax, -1.0, RED_NORM, FIN_STORE);
-      rr += read_state(ctx).sums[0];
-    }
+    const double rr = finish_solution(d64, kappa, clov, w.be, w.bo, w.x64, w.xe, w.aux, w.tmp64, nullptr);
     info.true_residual = std::sqrt(rr / bb);
     const bool relative_ok = prm.abs_tol || info.true_residual <= prm.tol;
     if (info.status != ST_CONVERGED || relative_ok || restart >= 12 || info.iterations >= prm.maxiter) {

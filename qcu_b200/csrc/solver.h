@@ -58,6 +58,31 @@ struct SolveInfo {
 // x, b: full two-parity spinors, PyQuda layout, complex128, device
 SolveInfo solve(GaugeHandle &G, void *x, const void *b, const SolveParams &p);
 
+int kind_of_precision(int prec);
+
+// One hopping-term application on a handle's fields in a given storage:
+//   out = a * [Ainv_par] D_{par <- 1-par} in + b1 x1 + b2 x2 (+ fused reduction)
+struct Dsl {
+  const GaugeHandle &G;
+  Context &ctx;
+  int kind;
+  int gkind = -1;  // gauge storage; -1: the one matching the spinor kind
+  void operator()(int par, const Spinor &in, Spinor &out, bool clover, double a, const Spinor *x1 = nullptr,
+                  double b1 = 0, const Spinor *x2 = nullptr, double b2 = 0, int red = RED_NONE, int fin = FIN_STORE,
+                  const Spinor *rt = nullptr, int gate = GATE_ALWAYS);
+};
+
+// b (PyQuda full spinor, device) -> be, bo (FP64 internal) and the even-odd
+// source bp = A_o^-1 (b_o + kappa D_oe A_e^-1 b_e); returns |b|^2.
+// (include/lattice_bistabcg.h:101-106 for the Wilson case)
+double prepare_source(Dsl &d64, const void *b_pyq, double kappa, bool clov, Spinor &be, Spinor &bo, Spinor &bp,
+                      Spinor &aux, Spinor &tmp64);
+// x_e = A_e^-1 (b_e + kappa D_eo x_o) and the full-system FP64 true |b - M x|^2;
+// also writes x (PyQuda layout) when x_pyq is not null
+// (include/lattice_bistabcg.h:313-332 for the Wilson case)
+double finish_solution(Dsl &d64, double kappa, bool clov, Spinor &be, Spinor &bo, Spinor &xo, Spinor &xe,
+                       Spinor &aux, Spinor &tmp64, void *x_pyq);
+
 // out = D_{par <- 1-par} in on PyQuda-layout half spinors (optionally A^-1 D),
 // computed in the given storage precision (64, 32, 16) on the packed gauge
 void handle_dslash(GaugeHandle &G, void *out, const void *in, int par, int use_clover, int precision);

@@ -1,0 +1,146 @@
+"""Micro-benchmarks of the library's hot path, for timing and profiling.
+
+    python -m qcu_b200.perf dslash --precision 32 --gauge-precision 16 --iters 5
+    python -m qcu_b200.perf solve  --precision 32 --gauge-precision 16
+    python -m qcu_b200.perf batch  --csw 1.0 --kappa 0.128
+
+`dslash` applies the even-odd hopping term `iters` times (after 3 warm-up
+launches) on a seeded smooth gauge field and prints the time per launch and
+the bandwidth of the algorithmic bytes (input spinor, 8 reconstruct-12 links,
+output spinor per site).  `solve` runs one solve of M x = b with the given
+solver settings and prints the solver report and its wall time.  `batch`
+solves, in one batched call, the 12 point sources of a propagator on the
+main lattice together with 4 Gaussian right-hand sides on each of
+16^3 x 32, 24^3 x 48 and a second gauge field of the main lattice, and
+prints the batched wall time next to the same 24 systems solved one at a
+time.  Inputs are
+generated on the GPU by the library's own generators; the working set of the
+default 32^3 x 64 lattice is larger than L2.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+# algorithmic bytes per output site of the hopping term, keyed by spinor/link precision
+DSLASH_BYTES = {(64, 64): 1152, (32, 32): 576, (16, 16): 296, (32, 16): 384}
+
+
+def _gauge(latt, eps, seed, t_bc, csw=0.0, kappa=0.0):
+    import torch
+
+    import qcu_b200 as q
+
+    L = q.Layout(tuple(latt))
+    u = torch.empty(L.gauge, dtype=torch.complex128, device="cuda")
+    q.gauge_random(u, latt, 1, eps, seed)
+    G = q.Gauge(u, latt, t_boundary=t_bc, clover_coeff=kappa * csw)
+    return G, u, L
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=["dslash", "solve", "batch"])
+    ap.add_argument("--latt", type=int, nargs=4, default=[32, 32, 32, 64])
+    ap.add_argument("--eps", type=float, default=0.25)
+    ap.add_argument("--seed", type=int, default=20251203)
+    ap.add_argument("--t-bc", type=float, default=-1.0)
+    ap.add_argument("--precision", type=int, default=32, choices=[16, 32, 64])
+    ap.add_argument("--gauge-precision", type=int, default=16, choices=[0, 16])
+    ap.add_argument("--clover", action="store_true", help="dslash: apply the inverse clover term too")
+    ap.add_argument("--csw", type=float, default=0.0)
+    ap.add_argument("--iters", type=int, default=20)
+    ap.add_argument("--kappa", type=float, default=0.1303)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--solver", default="gcr", choices=["gcr", "bicgstab"])
+    ap.add_argument("--inner-iters", type=int, default=96)
+    ap.add_argument("--inner-tol", type=float, default=0.05)
+    ap.add_argument("--gcr-k", type=int, default=4)
+    ap.add_argument("--single", action="store_true", help="batch: also time the 24 systems one at a time")
+    a = ap.parse_args(argv)
+    import torch
+
+    import qcu_b200 as q
+
+    gp = a.gauge_precision if a.gauge_precision else a.precision
+    if a.what == "dslash":
+        G, u, L = _gauge(a.latt, a.eps, a.seed, a.t_bc, a.csw if a.clover else 0.0, a.kappa)
+        del u
+        torch.cuda.empty_cache()
+        ms = G.bench_dslash(a.precision, a.clover, a.iters, gauge_precision=a.gauge_precision)
+        nb = DSLASH_BYTES[(a.precision, gp)] * L.vh
+        print(json.dumps({"kernel": "dslash", "latt": a.latt, "precision": a.precision, "gauge_precision": gp,
+                          "clover": a.clover, "ms": round(ms, 5), "bytes": nb,
+                          "GBps": round(nb / (ms * 1e-3) / 1e9, 1)}))
+        G.close()
+        return
+    if a.what == "batch":
+        _batch(a)
+        return
+    G, u, L = _gauge(a.latt, a.eps, a.seed, a.t_bc, a.csw, a.kappa)
+    b = torch.empty(L.full, dtype=torch.complex128, device="cuda")
+    q.fermion_random(b, b.numel(), 0, 7)
+    x = torch.empty_like(b)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    info = G.invert(x, b, a.kappa, tol=a.tol, maxiter=20000, precision=a.precision,
+                    gauge_precision=a.gauge_precision, solver=a.solver, inner_iters=a.inner_iters,
+                    inner_tol=a.inner_tol, gcr_k=a.gcr_k, clover=a.csw != 0.0)
+    torch.cuda.synchronize()
+    info["seconds"] = round(time.perf_counter() - t0, 4)
+    print(json.dumps(info))
+    G.close()
+
+
+def _batch(a):
+    import torch
+
+    import qcu_b200 as q
+
+    kw = dict(tol=a.tol, maxiter=20000, precision=a.precision, gauge_precision=a.gauge_precision,
+              inner_iters=a.inner_iters, inner_tol=a.inner_tol, gcr_k=a.gcr_k)
+    clov = a.csw != 0.0
+    systems, handles = [], []
+    G0, u, L0 = _gauge(a.latt, a.eps, a.seed, a.t_bc, a.csw, a.kappa)
+    del u
+    handles.append(G0)
+    b0 = q.point_sources(a.latt, [0, 0, 0, 0])
+    systems.append((G0, torch.empty_like(b0), b0, a.kappa, clov))
+    for i, latt in enumerate([[16, 16, 16, 32], [24, 24, 24, 48], list(a.latt)]):
+        G, u, L = _gauge(latt, a.eps, a.seed + 1 + i, a.t_bc, a.csw, a.kappa)
+        del u
+        handles.append(G)
+        b = torch.empty((4,) + L.full, dtype=torch.complex128, device="cuda")
+        q.fermion_random(b, b.numel(), 0, 100 + i)
+        systems.append((G, torch.empty_like(b), b, a.kappa, clov))
+    torch.cuda.empty_cache()
+    q.invert_batch(systems, **kw)  # first call of this shape: autotune, allocation
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res, tune = q.invert_batch(systems, **kw)
+    torch.cuda.synchronize()
+    tb = time.perf_counter() - t0
+    out = {"kernel": "batch", "rhs": len(res), "seconds": round(tb, 4), "tune": tune,
+           "iterations": [r["iterations"] for r in res], "status": sorted(set(r["status"] for r in res)),
+           "max_true_residual": max(r["true_residual"] for r in res)}
+    if a.single:
+        ts, it = 0.0, []
+        for G, x, b, kappa, cl in systems:
+            for j in range(b.shape[0]):
+                xj = torch.empty_like(b[j])
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                info = G.invert(xj, b[j].contiguous(), kappa, clover=cl, solver="gcr", **kw)
+                torch.cuda.synchronize()
+                ts += time.perf_counter() - t0
+                it.append(info["iterations"])
+        out["single_seconds"] = round(ts, 4)
+        out["single_iterations"] = it
+    print(json.dumps(out))
+    for G in handles:
+        G.close()
+
+
+if __name__ == "__main__":
+    main()
