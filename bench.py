@@ -41,6 +41,8 @@ SRC_SEED = 7
 KAPPA = 0.1303            # plain FP64 BiCGSTAB: 620 iterations on this ensemble (0.1304: no convergence in 4000)
 PLAIN_ITERS_REF = 620     # plain FP64 iterations of this system (measured), used to extrapolate CPU samples
 TOL = 1e-10
+CSW = 1.0
+KAPPA_CLOVER = 0.1291     # clover csw = 1 on the same field: near-critical (plain FP64 ~1000 iterations)
 METRIC = "solve s to 1e-10 true residual, chosen vs plain FP64, 1 B200; dslash HBM GB/s"
 # algorithmic bytes per output site of the hopping term (in-spinor + 8 recon-12 links + out-spinor)
 DSLASH_BYTES = {"64": 192 + 8 * 96 + 192, "32": 96 + 8 * 48 + 96, "16": 52 + 8 * 24 + 52, "32/16": 96 + 8 * 24 + 96}
@@ -67,6 +69,7 @@ def parse():
     ap.add_argument("--latt", type=int, nargs=4, default=LATT)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the clover and batched measurements")
     return ap.parse_args()
 
 
@@ -211,6 +214,93 @@ def run_reference(args, world, rank, pg):
     print(json.dumps(line), flush=True)
 
 
+def event_time(stream, fn):
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3, out
+
+
+def clover_target(args, q, gauge, b, x, latt, stream, chosen_kw):
+    """Clover csw = 1 at near-critical kappa on the same field: plain FP64
+    BiCGSTAB vs the chosen solver (one timed solve each after a warm-up)."""
+    with q.Gauge(gauge, latt, t_boundary=T_BC, clover_coeff=KAPPA_CLOVER * CSW) as G:
+        def solve(**kw):
+            info = G.invert(x, b, KAPPA_CLOVER, tol=TOL, maxiter=20000, clover=True, **kw)
+            if info["status"] != 1 or info["true_residual"] > TOL:
+                raise RuntimeError(f"clover solve failed: {info}")
+            return info
+        solve(**chosen_kw)
+        tp, ip = event_time(stream, lambda: solve(precision=64, delta=0.0))
+        tc, ic = event_time(stream, lambda: solve(**chosen_kw))
+    return {"workload": f"wilson-clover-csw{CSW}-32^3x64-smooth-eps0.25", "kappa": KAPPA_CLOVER,
+            "plain_fp64": {"seconds": round(tp, 4), "iterations": ip["iterations"],
+                           "true_residual": ip["true_residual"]},
+            "chosen": {"seconds": round(tc, 4), "iterations": ic["iterations"], "outer_steps": ic["reliable_updates"],
+                       "true_residual": ic["true_residual"]},
+            "speedup_vs_plain_fp64": round(tp / tc, 3)}
+
+
+def batch_config(args, q, stream, chosen_kw):
+    """Batched multi-RHS workload: the 12 point sources of a propagator on
+    32^3 x 64 clover (csw = 1) together with 4 Gaussian right-hand sides on
+    each of 16^3 x 32, 24^3 x 48 and 32^3 x 64 (clover), one batched solve;
+    against the same 24 systems solved one at a time by the chosen solver and
+    by plain FP64 BiCGSTAB (one solve per system, times nrhs)."""
+    import torch
+
+    kw = {k: chosen_kw[k] for k in ("precision", "gauge_precision", "inner_iters", "inner_tol", "gcr_k")}
+    systems, handles, plain, single = [], [], 0.0, 0.0
+    shapes = [(LATT, "point12"), ([16, 16, 16, 32], 4), ([24, 24, 24, 48], 4), (LATT, 4)]
+    try:
+        for i, (lt, what) in enumerate(shapes):
+            L = q.Layout(tuple(lt))
+            u = torch.empty(L.gauge, dtype=torch.complex128, device="cuda")
+            q.gauge_random(u, lt, 1, EPS, GAUGE_SEED + 11 * i)
+            G = q.Gauge(u, lt, t_boundary=T_BC, clover_coeff=KAPPA_CLOVER * CSW)
+            del u
+            handles.append(G)
+            if what == "point12":
+                bb = q.point_sources(lt, [0, 0, 0, 0])
+            else:
+                bb = torch.empty((what,) + L.full, dtype=torch.complex128, device="cuda")
+                q.fermion_random(bb, bb.numel(), 0, SRC_SEED + 100 + i)
+            systems.append((G, torch.empty_like(bb), bb, KAPPA_CLOVER, True))
+        torch.cuda.empty_cache()
+        res, tune = q.invert_batch(systems, tol=TOL, maxiter=20000, **kw)  # autotune + allocation
+        tb, (res, tune) = event_time(stream, lambda: q.invert_batch(systems, tol=TOL, maxiter=20000, **kw))
+        for r in res:
+            if r["status"] != 1 or r["true_residual"] > TOL:
+                raise RuntimeError(f"batched solve failed: {r}")
+        for G, x, bb, kappa, cl in systems:
+            xs = torch.empty_like(bb[0])
+            b0 = bb[0].contiguous()
+            tp, ip = event_time(stream, lambda: G.invert(xs, b0, kappa, tol=TOL, maxiter=20000, precision=64,
+                                                         delta=0.0, clover=True))
+            plain += tp * bb.shape[0]
+            for j in range(bb.shape[0]):
+                bj = bb[j].contiguous()
+                tj, _ = event_time(stream, lambda: G.invert(xs, bj, kappa, tol=TOL, maxiter=20000, clover=True,
+                                                            solver="gcr", **kw))
+                single += tj
+    finally:
+        for G in handles:
+            G.close()
+    return {"workload": "propagator (12 point sources) 32^3x64 + 4 rhs each on 16^3x32, 24^3x48, 32^3x64; "
+                        f"clover csw {CSW}, kappa {KAPPA_CLOVER}",
+            "rhs": len(res), "seconds": round(tb, 4), "tune": tune,
+            "iterations_max": max(r["iterations"] for r in res),
+            "max_true_residual": max(r["true_residual"] for r in res),
+            "one_at_a_time_chosen_seconds": round(single, 4),
+            "plain_fp64_seconds_estimate": round(plain, 4),
+            "speedup_vs_one_at_a_time": round(single / tb, 3),
+            "speedup_vs_plain_fp64": round(plain / tb, 3)}
+
+
 def run_ours(args, world, rank, local, pg):
     import numpy as np
     import torch
@@ -320,6 +410,11 @@ def run_ours(args, world, rank, local, pg):
         e2e = {"value": round(e2e_t, 4), "unit": "s", "h2d_bytes_per_step": hg.numel() * 16 + hb.numel() * 16,
                "d2h_bytes_per_step": hx.numel() * 16}
 
+    extra = {}
+    if not args.no_extra and latt == LATT:
+        extra["clover_target"] = clover_target(args, q, gauge, b, x, latt, lib_stream, chosen_kw)
+        extra["batch"] = batch_config(args, q, lib_stream, chosen_kw)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_sample(latt, args.kappa, gauge.cpu().numpy(), b.cpu().numpy(), plain_info["iterations"])
@@ -349,6 +444,7 @@ def run_ours(args, world, rank, local, pg):
             "dslash": {k: {"ms": round(v["ms"], 4), "GBps": round(v["GBps"], 1), "frac_of_peak": round(v["GBps"] / pk, 4),
                            "TFLOPs": round(v["TFLOPs"], 2)} for k, v in dsl.items()},
             "roofline": roofline,
+            **extra,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches),

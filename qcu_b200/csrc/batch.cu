@@ -8,63 +8,11 @@
 // scalars and lattice: in the descriptor of its rhs.  Reductions end in the
 // last block of the rhs's own tiles (per-rhs ticket, fixed summation order,
 // so results are deterministic and independent of the other rhs).
-#include "batch.h"
+#include <algorithm>
+
+#include "batch_dev.cuh"
 
 namespace qcu {
-
-template <int K>
-using Real = typename SpinorReal<K>::T;
-
-__device__ __forceinline__ bool bgate(const BatchArgs &a, int rhs, int gate) {
-  if (gate == BG_ALWAYS) return true;
-  if (gate == BG_ACTIVE) return a.active[rhs] != 0;
-  return ((volatile const SolverState *)(a.st + rhs))->done == 0;
-}
-
-// block partial of one rhs -> its partials; the last of its tiles sums them
-// in tile order and applies the finalize op to that rhs's state
-template <int NV, int BS>
-__device__ __forceinline__ void batch_reduce(double v[NV], const BatchArgs &a, int rhs, int b, int op) {
-  __shared__ bool last;
-  double part[NV];
-  block_sum<NV, BS>(v, part);
-  const RhsDesc &d = a.d[rhs];
-  double *P = a.partials + (size_t)d.poff[a.table] * RED_MAXV;
-  const int n = d.ntile[a.table];
-  SolverState *st = a.st + rhs;
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; k++) P[(size_t)b * RED_MAXV + k] = part[k];
-    __threadfence();
-    const unsigned t = atomicAdd(&st->ticket, 1u);
-    last = (t == (unsigned)n - 1u);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  double acc[NV];
-#pragma unroll
-  for (int k = 0; k < NV; k++) acc[k] = 0.0;
-  for (int q = threadIdx.x; q < n; q += BS) {
-#pragma unroll
-    for (int k = 0; k < NV; k++) acc[k] += ((volatile double *)P)[(size_t)q * RED_MAXV + k];
-  }
-  double tot[NV];
-  block_sum<NV, BS>(acc, tot);
-  if (threadIdx.x == 0) {
-    double s[RED_MAXV];
-#pragma unroll
-    for (int k = 0; k < RED_MAXV; k++) s[k] = k < NV ? tot[k] : 0.0;
-    finalize(st, op, s);
-    st->ticket = 0;
-    __threadfence();
-  }
-}
-
-template <int K>
-__device__ __forceinline__ SpinorView<K> bview(const RhsDesc &d, int role) {
-  return SpinorView<K>{d.v[role], d.vn[role], d.g.Vh};
-}
 
 // ---------------------------------------------------------------- hopping term
 // One hop for the NR right-hand sides of a group: the link is loaded (and
@@ -87,14 +35,15 @@ __device__ __forceinline__ void hop_group(Cpx<T> (&acc)[NR][12], const SpinorVie
       for (int k = 0; k < 9; k++) u[k] = u[k] * ph;
     }
   }
+  // every slot is computed (a closed or empty slot reads a valid buffer and
+  // is discarded in the epilogue): no branch between the loads of the slots
 #pragma unroll
   for (int j = 0; j < NR; j++) {
-    if (on[j]) {
-      Cpx<T> psi[12];
-      spinor_load<K, T>(in[j], n, psi);
-      hop<MU, FWD, false, T>(acc[j], psi, u, T(1));
-    }
+    Cpx<T> psi[12];
+    spinor_load<K, T>(in[j], n, psi);
+    hop<MU, FWD, false, T>(acc[j], psi, u, T(1));
   }
+  (void)on;
 }
 
 template <int K, int G, typename T, int NR>
@@ -137,10 +86,9 @@ __device__ __forceinline__ void wilson_hop_group(Cpx<T> (&acc)[NR][12], const Sp
 // computes its site for all open rhs of the group, then the epilogue and the
 // per-rhs reductions rhs by rhs.
 template <int K, int G, bool CLOV, int NX, int RED, int NT, int NR>
-__global__ void __launch_bounds__(NT, BDSL_MIN_BLOCKS(K, NT, NR)) kb_dslash(BatchArgs a, BDslOp op) {
+__device__ __forceinline__ void kb_dslash_tile(const BatchArgs &a, const int2 tile, BDslOp op) {
   using T = Real<K>;
   constexpr int C = K == SOA64 ? CSOA64 : CSOA32;
-  const int2 tile = a.tiles[blockIdx.x];
   const RhsGroup grp = a.groups[tile.x];
   bool on[NR];
   bool any = false;
@@ -163,7 +111,7 @@ __global__ void __launch_bounds__(NT, BDSL_MIN_BLOCKS(K, NT, NR)) kb_dslash(Batc
     Cpx<T> w[NR][12];
     SpinorView<K> in[NR];
 #pragma unroll
-    for (int j = 0; j < NR; j++) in[j] = bview<K>(a.d[grp.rhs[on[j] ? j : 0]], op.in);
+    for (int j = 0; j < NR; j++) in[j] = bview<K>(a.d[grp.rhs[j]], op.in);  // empty slots repeat the first rhs
     const GaugeView<G> U{K == SOA64 ? d0.g64 : d0.gin, pad_sites(g.Vh)};
     wilson_hop_group<K, G, T, NR>(w, in, on, U, g, s, op.parity, (T)d0.t_bc);
     const void *cl = CLOV ? (K == SOA64 ? d0.c64[op.parity] : d0.cin[op.parity]) : nullptr;
@@ -228,9 +176,8 @@ constexpr int BB = 128;  // threads per BLAS tile
 
 // p = r + beta (p - omega v),  beta = (rho/rho_prev)(alpha/omega)
 template <int K>
-__global__ void __launch_bounds__(BB) kb_pupdate(BatchArgs a) {
+__device__ __forceinline__ void kb_pupdate_tile(const BatchArgs &a, const int2 tile) {
   using T = Real<K>;
-  const int2 tile = a.tiles[blockIdx.x];
   if (!bgate(a, tile.x, BG_NOT_DONE)) return;
   const RhsDesc &d = a.d[tile.x];
   SolverState *st = a.st + tile.x;
@@ -256,9 +203,8 @@ __global__ void __launch_bounds__(BB) kb_pupdate(BatchArgs a) {
 
 // s = r - alpha v
 template <int K>
-__global__ void __launch_bounds__(BB) kb_supdate(BatchArgs a) {
+__device__ __forceinline__ void kb_supdate_tile(const BatchArgs &a, const int2 tile) {
   using T = Real<K>;
-  const int2 tile = a.tiles[blockIdx.x];
   if (!bgate(a, tile.x, BG_NOT_DONE)) return;
   const RhsDesc &d = a.d[tile.x];
   const SolverState *st = a.st + tile.x;
@@ -276,10 +222,9 @@ __global__ void __launch_bounds__(BB) kb_supdate(BatchArgs a) {
 
 // x += alpha p + omega s ; r = s - omega t ; <rt, r>, |r|^2 -> FIN_XR
 template <int K, int XK>
-__global__ void __launch_bounds__(BB) kb_xrupdate(BatchArgs a) {
+__device__ __forceinline__ void kb_xrupdate_tile(const BatchArgs &a, const int2 tile) {
   using T = Real<K>;
   using TX = Real<XK>;
-  const int2 tile = a.tiles[blockIdx.x];
   if (!bgate(a, tile.x, BG_NOT_DONE)) return;
   const RhsDesc &d = a.d[tile.x];
   const SolverState *st = a.st + tile.x;
@@ -317,10 +262,9 @@ __global__ void __launch_bounds__(BB) kb_xrupdate(BatchArgs a) {
 // r = rt = r64, p = v = x = 0 ; <rt, r>, |r64|^2 -> FIN_INIT.  An inactive
 // rhs reduces zeros, which FIN_INIT (inner mode) turns into "done".
 template <int K, int XK>
-__global__ void __launch_bounds__(BB) kb_init(BatchArgs a) {
+__device__ __forceinline__ void kb_init_tile(const BatchArgs &a, const int2 tile) {
   using T = Real<K>;
   using TX = Real<XK>;
-  const int2 tile = a.tiles[blockIdx.x];
   const RhsDesc &d = a.d[tile.x];
   double red[3] = {0, 0, 0};
   if (a.active[tile.x]) {
@@ -350,9 +294,8 @@ __global__ void __launch_bounds__(BB) kb_init(BatchArgs a) {
 
 // z = x in FP64 (active rhs)
 template <int XK>
-__global__ void __launch_bounds__(BB) kb_xout(BatchArgs a) {
+__device__ __forceinline__ void kb_xout_tile(const BatchArgs &a, const int2 tile) {
   using TX = Real<XK>;
-  const int2 tile = a.tiles[blockIdx.x];
   if (!bgate(a, tile.x, BG_ACTIVE)) return;
   const RhsDesc &d = a.d[tile.x];
   BTILE_SITES(a, tile, d)
@@ -403,8 +346,7 @@ __device__ __forceinline__ void st64(void *p, int s, const C v[12]) {
 }
 
 // sums[2j], sums[2j+1] = <W_j, w>, j < k
-__global__ void __launch_bounds__(BB) kb_gcr_multidot(BatchArgs a, int k) {
-  const int2 tile = a.tiles[blockIdx.x];
+__device__ __forceinline__ void kb_gcr_multidot_tile(const BatchArgs &a, const int2 tile, int k) {
   if (!bgate(a, tile.x, BG_ACTIVE)) return;
   const RhsDesc &d = a.d[tile.x];
   double red[2 * GCR_MAXK];
@@ -431,8 +373,7 @@ __global__ void __launch_bounds__(BB) kb_gcr_multidot(BatchArgs a, int k) {
 }
 
 // W_k = w - sum beta_j W_j, Z_k = z - sum beta_j Z_j ; sums = |W_k|^2, <W_k, r>
-__global__ void __launch_bounds__(BB) kb_gcr_orth(BatchArgs a, int k) {
-  const int2 tile = a.tiles[blockIdx.x];
+__device__ __forceinline__ void kb_gcr_orth_tile(const BatchArgs &a, const int2 tile, int k) {
   if (!bgate(a, tile.x, BG_ACTIVE)) return;
   const RhsDesc &d = a.d[tile.x];
   const BatchCoef &cf = a.coef[tile.x];
@@ -466,8 +407,7 @@ __global__ void __launch_bounds__(BB) kb_gcr_orth(BatchArgs a, int k) {
 }
 
 // x64 += alpha Z_k ; r64 -= alpha W_k ; sums[0] = |r64|^2
-__global__ void __launch_bounds__(BB) kb_gcr_update(BatchArgs a, int k) {
-  const int2 tile = a.tiles[blockIdx.x];
+__device__ __forceinline__ void kb_gcr_update_tile(const BatchArgs &a, const int2 tile, int k) {
   if (!bgate(a, tile.x, BG_ACTIVE)) return;
   const RhsDesc &d = a.d[tile.x];
   const C al(a.coef[tile.x].alpha[0], a.coef[tile.x].alpha[1]);
@@ -492,20 +432,78 @@ __global__ void __launch_bounds__(BB) kb_gcr_update(BatchArgs a, int k) {
   batch_reduce<1, BB>(red, a, tile.x, tile.y, FIN_STORE);
 }
 
+// ---------------------------------------------------------------- persistent wrappers
+// Each kernel loops over the tile table with a grid of resident blocks: a tile
+// of a converged rhs costs a few instructions instead of a block launch.
+template <int K, int G, bool CLOV, int NX, int RED, int NT, int NR>
+__global__ void __launch_bounds__(NT, BDSL_MIN_BLOCKS(K, NT, NR)) kb_dslash(BatchArgs a, BDslOp op) {
+  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_dslash_tile<K, G, CLOV, NX, RED, NT, NR>(a, a.tiles[k], op);
+}
+
+template <int K>
+__global__ void __launch_bounds__(BB) kb_pupdate(BatchArgs a) {
+  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_pupdate_tile<K>(a, a.tiles[k]);
+}
+
+template <int K>
+__global__ void __launch_bounds__(BB) kb_supdate(BatchArgs a) {
+  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_supdate_tile<K>(a, a.tiles[k]);
+}
+
+template <int K, int XK>
+__global__ void __launch_bounds__(BB) kb_xrupdate(BatchArgs a) {
+  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_xrupdate_tile<K, XK>(a, a.tiles[k]);
+}
+
+template <int K, int XK>
+__global__ void __launch_bounds__(BB) kb_init(BatchArgs a) {
+  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_init_tile<K, XK>(a, a.tiles[k]);
+}
+
+template <int XK>
+__global__ void __launch_bounds__(BB) kb_xout(BatchArgs a) {
+  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_xout_tile<XK>(a, a.tiles[k]);
+}
+
+__global__ void __launch_bounds__(BB) kb_gcr_multidot(BatchArgs a, int k) {
+  for (int q = blockIdx.x; q < a.ntiles; q += gridDim.x) kb_gcr_multidot_tile(a, a.tiles[q], k);
+}
+
+__global__ void __launch_bounds__(BB) kb_gcr_orth(BatchArgs a, int k) {
+  for (int q = blockIdx.x; q < a.ntiles; q += gridDim.x) kb_gcr_orth_tile(a, a.tiles[q], k);
+}
+
+__global__ void __launch_bounds__(BB) kb_gcr_update(BatchArgs a, int k) {
+  for (int q = blockIdx.x; q < a.ntiles; q += gridDim.x) kb_gcr_update_tile(a, a.tiles[q], k);
+}
+
 // ---------------------------------------------------------------- launchers
+// Grid of a persistent batched kernel: as many blocks as the SMs can hold by
+// thread count (or fewer when the table has fewer tiles); each block then
+// walks the tile table with a stride of the grid.
+static int persistent_grid(const BatchArgs &a, int threads) {
+  const int cap = std::max(1, a.sms) * std::max(1, 2048 / threads);
+  return std::max(1, std::min(a.ntiles, cap));
+}
 template <int K, int G, bool CLOV, int NT, int NR>
 static void bdsl_nx(const BatchArgs &a, const BDslOp &op, cudaStream_t s) {
   const int nx = op.x2 >= 0 ? 2 : (op.x1 >= 0 ? 1 : 0);
-  const dim3 grid(a.ntiles), block(NT);
-#define QCU_BD(NX, RED) kb_dslash<K, G, CLOV, NX, RED, NT, NR><<<grid, block, 0, s>>>(a, op)
+#define QCU_BD(NX, RED) kb_dslash<K, G, CLOV, NX, RED, NT, NR><<<persistent_grid(a, NT), NT, 0, s>>>(a, op)
   // the combinations the batched solver uses: inner (0,-), (1,<rt,v>), (1,<t,s>|t|^2);
-  // FP64 (0,-), (1,-), (2,|r|^2)
-  if (nx == 0 && op.red == RED_NONE) QCU_BD(0, RED_NONE);
-  else if (K != SOA64 && nx == 1 && op.red == RED_DOT_RT) QCU_BD(1, RED_DOT_RT);
-  else if (K != SOA64 && nx == 1 && op.red == RED_TS_TT) QCU_BD(1, RED_TS_TT);
-  else if (K == SOA64 && nx == 1 && op.red == RED_NONE) QCU_BD(1, RED_NONE);
-  else if (K == SOA64 && nx == 2 && op.red == RED_NORM) QCU_BD(2, RED_NORM);
-  else throw Error(1, "batched dslash: unsupported epilogue/reduction combination");
+  // FP64 outer (0,-), (1,-), (2,|r|^2)
+  if (nx == 0 && op.red == RED_NONE) {
+    QCU_BD(0, RED_NONE);
+  } else if constexpr (K == SOA64) {  // outer operator, and the inner one at precision 64
+    if (nx == 1 && op.red == RED_NONE) QCU_BD(1, RED_NONE);
+    else if (nx == 2 && op.red == RED_NORM) QCU_BD(2, RED_NORM);
+    else if (nx == 1 && op.red == RED_DOT_RT) QCU_BD(1, RED_DOT_RT);
+    else if (nx == 1 && op.red == RED_TS_TT) QCU_BD(1, RED_TS_TT);
+    else throw Error(1, "batched FP64 dslash: unsupported epilogue/reduction combination");
+  } else {
+    if (nx == 1 && op.red == RED_DOT_RT) QCU_BD(1, RED_DOT_RT);
+    else if (nx == 1 && op.red == RED_TS_TT) QCU_BD(1, RED_TS_TT);
+    else throw Error(1, "batched dslash: unsupported epilogue/reduction combination");
+  }
 #undef QCU_BD
   QCU_CHECK_LAUNCH();
 }
@@ -537,13 +535,13 @@ static void bdsl_shape(const BatchArgs &a, const BDslOp &op, const BatchTune &t,
   }
 }
 
-void launch_bdslash_mma(int gkind, const BatchArgs &a, const BDslOp &op, cudaStream_t s);
+void launch_bdslash_mma(int gkind, int mode, const BatchArgs &a, const BDslOp &op, cudaStream_t s);
 
 void launch_bdslash(int kind, int gkind, const BatchArgs &a, const BDslOp &op, const BatchTune &t, cudaStream_t s) {
   if (a.ntiles == 0) return;
   if (t.mma) {
     require(kind == SOA32, "tensor-core dslash: FP32 spinors only");
-    launch_bdslash_mma(gkind, a, op, s);
+    launch_bdslash_mma(gkind, t.mma, a, op, s);
     return;
   }
   if (kind == SOA64 && gkind == GSOA64) bdsl_shape<SOA64, GSOA64>(a, op, t, s);
@@ -553,28 +551,28 @@ void launch_bdslash(int kind, int gkind, const BatchArgs &a, const BDslOp &op, c
 }
 
 void launch_bpupdate(int kind, const BatchArgs &a, cudaStream_t s) {
-  if (kind == SOA64) kb_pupdate<SOA64><<<a.ntiles, BB, 0, s>>>(a);
-  else kb_pupdate<SOA32><<<a.ntiles, BB, 0, s>>>(a);
+  if (kind == SOA64) kb_pupdate<SOA64><<<persistent_grid(a, BB), BB, 0, s>>>(a);
+  else kb_pupdate<SOA32><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   QCU_CHECK_LAUNCH();
 }
 void launch_bsupdate(int kind, const BatchArgs &a, cudaStream_t s) {
-  if (kind == SOA64) kb_supdate<SOA64><<<a.ntiles, BB, 0, s>>>(a);
-  else kb_supdate<SOA32><<<a.ntiles, BB, 0, s>>>(a);
+  if (kind == SOA64) kb_supdate<SOA64><<<persistent_grid(a, BB), BB, 0, s>>>(a);
+  else kb_supdate<SOA32><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   QCU_CHECK_LAUNCH();
 }
 void launch_bxrupdate(int kind, const BatchArgs &a, cudaStream_t s) {
-  if (kind == SOA64) kb_xrupdate<SOA64, SOA64><<<a.ntiles, BB, 0, s>>>(a);
-  else kb_xrupdate<SOA32, SOA32><<<a.ntiles, BB, 0, s>>>(a);
+  if (kind == SOA64) kb_xrupdate<SOA64, SOA64><<<persistent_grid(a, BB), BB, 0, s>>>(a);
+  else kb_xrupdate<SOA32, SOA32><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   QCU_CHECK_LAUNCH();
 }
 void launch_binit(int kind, const BatchArgs &a, cudaStream_t s) {
-  if (kind == SOA64) kb_init<SOA64, SOA64><<<a.ntiles, BB, 0, s>>>(a);
-  else kb_init<SOA32, SOA32><<<a.ntiles, BB, 0, s>>>(a);
+  if (kind == SOA64) kb_init<SOA64, SOA64><<<persistent_grid(a, BB), BB, 0, s>>>(a);
+  else kb_init<SOA32, SOA32><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   QCU_CHECK_LAUNCH();
 }
 void launch_bxout(int kind, const BatchArgs &a, cudaStream_t s) {
-  if (kind == SOA64) kb_xout<SOA64><<<a.ntiles, BB, 0, s>>>(a);
-  else kb_xout<SOA32><<<a.ntiles, BB, 0, s>>>(a);
+  if (kind == SOA64) kb_xout<SOA64><<<persistent_grid(a, BB), BB, 0, s>>>(a);
+  else kb_xout<SOA32><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   QCU_CHECK_LAUNCH();
 }
 void launch_bloop_cond(const BatchArgs &a, cudaGraphConditionalHandle h, unsigned cap, cudaStream_t s) {
@@ -583,15 +581,15 @@ void launch_bloop_cond(const BatchArgs &a, cudaGraphConditionalHandle h, unsigne
   QCU_CHECK_LAUNCH();
 }
 void launch_bgcr_multidot(const BatchArgs &a, int k, cudaStream_t s) {
-  kb_gcr_multidot<<<a.ntiles, BB, 0, s>>>(a, k);
+  kb_gcr_multidot<<<persistent_grid(a, BB), BB, 0, s>>>(a, k);
   QCU_CHECK_LAUNCH();
 }
 void launch_bgcr_orth(const BatchArgs &a, int k, cudaStream_t s) {
-  kb_gcr_orth<<<a.ntiles, BB, 0, s>>>(a, k);
+  kb_gcr_orth<<<persistent_grid(a, BB), BB, 0, s>>>(a, k);
   QCU_CHECK_LAUNCH();
 }
 void launch_bgcr_update(const BatchArgs &a, int k, cudaStream_t s) {
-  kb_gcr_update<<<a.ntiles, BB, 0, s>>>(a, k);
+  kb_gcr_update<<<persistent_grid(a, BB), BB, 0, s>>>(a, k);
   QCU_CHECK_LAUNCH();
 }
 

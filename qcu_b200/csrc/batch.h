@@ -70,6 +70,7 @@ struct BatchArgs {
   int table = 0;                  // BatchTable of `tiles`
   int ntiles = 0;
   int tile_sites = 128;           // sites per tile
+  int sms = 148;                  // SMs of the device (grid of the persistent kernels)
 };
 
 // One batched hopping-term application:
@@ -86,10 +87,10 @@ struct BDslOp {
 
 // tunables chosen per batch shape by the autotuner
 struct BatchTune {
-  int dslash_threads = 128;  // threads (= sites) per dslash tile: 64, 128 or 256
+  int dslash_threads = 128;  // sites per dslash tile: 64, 128 or 256 (one thread each); 32 for the tensor-core path
   int dslash_rhs = 1;        // right-hand sides per dslash thread: 1, 2 or 4 (8 rhs per warp: tensor cores)
   int blas_sites = 256;      // sites per BLAS tile (128 threads each)
-  int mma = 0;               // 1: tensor-core contraction for the inner dslash
+  int mma = 0;               // tensor-core contraction for the inner dslash: 1 3xTF32 (FP32-accurate), 2 TF32
 };
 
 void launch_bdslash(int kind, int gkind, const BatchArgs &a, const BDslOp &op, const BatchTune &t, cudaStream_t s);

@@ -110,6 +110,8 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
   std::lock_guard<std::mutex> lk(ctx.mu);
   cudaStream_t st = ctx.stream;
   BatchCache &c = cache();
+  int sms = 0;
+  QCU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
   QCU_CUDA(cudaDeviceSynchronize());  // inputs written on any stream are complete
 
   // ---- buffers and sources
@@ -167,9 +169,9 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
       d.Z[k] = B.Z[k].data.p;
     }
   }
-  // partials: enough for the finest table any candidate uses (64 sites per tile)
+  // partials: enough for the finest table any candidate uses (32 sites per tile)
   size_t max_tiles = 0;
-  for (int r = 0; r < R; r++) max_tiles += (Vh[r] + 63) / 64;
+  for (int r = 0; r < R; r++) max_tiles += (Vh[r] + 31) / 32;
   c.partials.ensure(max_tiles * RED_MAXV * sizeof(double));
   c.st.ensure(sizeof(SolverState) * BATCH_MAX_RHS);
   c.active.ensure(sizeof(int) * BATCH_MAX_RHS);
@@ -180,9 +182,20 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
   key << kind << "/" << gkind;
   for (int r = 0; r < R; r++) key << ":" << Vh[r] << (rl[r].s->use_clover ? "c" : "");
   const auto found = c.tuned.find(key.str());
-  const bool need_tune = found == c.tuned.end() && kind == SOA32;
+  bool need_tune = found == c.tuned.end() && kind == SOA32;
   BatchTune tune;
   if (found != c.tuned.end()) tune = found->second;
+  // QCU_BATCH_TUNE="threads,rhs,blas_sites,mma" fixes the tunables (no autotuning)
+  if (const char *fix = getenv("QCU_BATCH_TUNE")) {
+    BatchTune f;
+    require(sscanf(fix, "%d,%d,%d,%d", &f.dslash_threads, &f.dslash_rhs, &f.blas_sites, &f.mma) == 4,
+            "QCU_BATCH_TUNE must be threads,rhs,blas_sites,mma");
+    require(f.blas_sites >= 128 && f.blas_sites % 128 == 0, "QCU_BATCH_TUNE: blas_sites must be a multiple of 128");
+    require(f.dslash_rhs >= 1 && f.dslash_rhs <= BATCH_MAX_NR, "QCU_BATCH_TUNE: rhs per group out of range");
+    tune = f;
+    need_tune = false;
+  }
+  const bool tune_log = getenv("QCU_TUNE_LOG") != nullptr;
   if (kind == SOA64) tune.dslash_threads = 128, tune.dslash_rhs = 1, tune.mma = 0;
 
   // rhs groups of the inner dslash (tune.dslash_rhs consecutive rhs of one
@@ -238,6 +251,7 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
       a.table = t;
       a.ntiles = (int)tiles.size();
       a.tile_sites = sites[t];
+      a.sms = sms;
       QCU_CUDA(cudaStreamSynchronize(st));  // the host tables die with this iteration
     }
     QCU_CUDA(cudaMemcpyAsync(c.desc.p, desc.data(), sizeof(RhsDesc) * R, cudaMemcpyHostToDevice, st));
@@ -306,9 +320,9 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
     op.in = BV_R, op.out = BV_TMP, op.parity = 0, op.clover = clov_any;
     BatchTune best = tune;
     double tbest = 1e30;
-    // (threads per block, rhs per thread, tensor-core path)
+    // (sites per tile, rhs per group, tensor-core path)
     const int cand[][3] = {{64, 1, 0},  {128, 1, 0}, {256, 1, 0}, {64, 2, 0},
-                           {128, 2, 0}, {64, 4, 0},  {128, 4, 0}, {128, 8, 1}};
+                           {128, 2, 0}, {64, 4, 0},  {128, 4, 0}, {32, 8, 1}};
     for (const auto &cd : cand) {
       tune.dslash_threads = cd[0];
       tune.dslash_rhs = cd[1];
@@ -320,6 +334,7 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
       } catch (const Error &) {
         cudaGetLastError();  // variant not available for this storage
       }
+      if (tune_log) fprintf(stderr, "qcu batch tune: dslash threads %d rhs %d mma %d: %.4f ms\n", cd[0], cd[1], cd[2], ms);
       if (ms < tbest) {
         tbest = ms;
         best.dslash_threads = cd[0];
@@ -333,6 +348,7 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
       tune.blas_sites = bs;
       build_tables();
       const double ms = time_it([&]() { launch_bsupdate(kind, A[BT_BLAS], st); });
+      if (tune_log) fprintf(stderr, "qcu batch tune: blas sites %d: %.4f ms\n", bs, ms);
       if (ms < tbest) {
         tbest = ms;
         best.blas_sites = bs;

@@ -33,6 +33,7 @@ GaugeHandle *gauge_load(const void *gauge_pyq, const int latt[4], double t_bc, d
   require(gauge_pyq != nullptr, "gauge pointer is null");
   require(t_bc == 1.0 || t_bc == -1.0, "t boundary must be +1 or -1");
   Context &ctx = context();
+  QCU_CUDA(cudaDeviceSynchronize());  // the field may still be in flight on another stream (an async copy)
   auto *G = new GaugeHandle();
   try {
     for (int d = 0; d < 4; d++) G->latt[d] = latt[d];

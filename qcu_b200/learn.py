@@ -21,13 +21,14 @@ import time
 import numpy as np
 
 
-def make_pairs(G, kappa: float, n_src: int, checkpoints, seed: int = 1, n_random: int = -1):
+def make_pairs(G, kappa: float, n_src: int, checkpoints, seed: int = 1, n_random: int = -1, clover: bool = False):
     """Returns (r, e): complex64 tensors [pairs, Vh, 4, 3] on the GPU.
 
     Solver-iterate errors concentrate on the low modes; on their own they
     teach the network to amplify, which hurts on the rough part of a
     residual.  n_random pairs with white-noise errors (default: as many as
-    the solver pairs) make the loss also cover |N M - 1| on every mode."""
+    the solver pairs) make the loss also cover |N M - 1| on every mode.
+    clover: pairs of the clover operator (G must carry a clover term)."""
     import torch
 
     import qcu_b200 as q
@@ -41,21 +42,21 @@ def make_pairs(G, kappa: float, n_src: int, checkpoints, seed: int = 1, n_random
     rs, es = [], []
     for i in range(n_src):
         q.fermion_random(b, b.numel(), 0, seed + i)
-        info = G.invert(xs, b, kappa, tol=1e-12, maxiter=20000, precision=64, delta=0.0)
+        info = G.invert(xs, b, kappa, tol=1e-12, maxiter=20000, precision=64, delta=0.0, clover=clover)
         if info["status"] != 1:
             raise RuntimeError(f"training solve failed: {info}")
         for k in checkpoints:
-            G.invert(xk, b, kappa, tol=1e-30, maxiter=int(k), precision=64, delta=0.0)
+            G.invert(xk, b, kappa, tol=1e-30, maxiter=int(k), precision=64, delta=0.0, clover=clover)
             e.copy_(xs[1] - xk[1])
             if float(torch.linalg.vector_norm(e)) == 0.0:
                 continue  # the iterate is already the solution to the last bit
-            G.matpc(r, e, kappa)
+            G.matpc(r, e, kappa, clover=clover)
             rs.append(r.to(torch.complex64).clone())
             es.append(e.to(torch.complex64).clone())
     n_random = len(rs) if n_random < 0 else n_random
     for i in range(n_random):
         q.fermion_random(e, e.numel(), 0, seed + 100000 + i)
-        G.matpc(r, e, kappa)
+        G.matpc(r, e, kappa, clover=clover)
         rs.append(r.to(torch.complex64).clone())
         es.append(e.to(torch.complex64).clone())
     return torch.stack(rs), torch.stack(es)
@@ -88,6 +89,7 @@ def main():
     ap.add_argument("--latt", type=int, nargs=4, default=[16, 16, 16, 16])
     ap.add_argument("--eps", type=float, default=0.25)
     ap.add_argument("--kappa", type=float, default=0.1303)
+    ap.add_argument("--csw", type=float, default=0.0, help="clover coefficient (0: Wilson)")
     ap.add_argument("--gauge-seed", type=int, default=4242)
     ap.add_argument("--sources", type=int, default=100)
     ap.add_argument("--checkpoints", type=int, nargs="+", default=[2, 4, 6, 8, 10, 12, 16, 20, 24, 28,
@@ -100,9 +102,9 @@ def main():
     L = q.Layout(tuple(args.latt))
     gauge = torch.empty(L.gauge, dtype=torch.complex128, device="cuda")
     q.gauge_random(gauge, args.latt, 1, args.eps, args.gauge_seed)
-    G = q.Gauge(gauge, args.latt, t_boundary=-1.0)
+    G = q.Gauge(gauge, args.latt, t_boundary=-1.0, clover_coeff=args.kappa * args.csw)
     t0 = time.time()
-    r, e = make_pairs(G, args.kappa, args.sources, args.checkpoints)
+    r, e = make_pairs(G, args.kappa, args.sources, args.checkpoints, clover=args.csw != 0.0)
     print(f"{r.shape[0]} pairs in {time.time() - t0:.1f} s", flush=True)
     net = q.Network(seed=1, init_scale=0.01)
     t0 = time.time()

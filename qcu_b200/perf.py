@@ -58,6 +58,7 @@ def main(argv=None):
     ap.add_argument("--inner-tol", type=float, default=0.05)
     ap.add_argument("--gcr-k", type=int, default=4)
     ap.add_argument("--single", action="store_true", help="batch: also time the 24 systems one at a time")
+    ap.add_argument("--only-point", action="store_true", help="batch: only the 12 point sources on --latt")
     a = ap.parse_args(argv)
     import torch
 
@@ -107,7 +108,7 @@ def _batch(a):
     handles.append(G0)
     b0 = q.point_sources(a.latt, [0, 0, 0, 0])
     systems.append((G0, torch.empty_like(b0), b0, a.kappa, clov))
-    for i, latt in enumerate([[16, 16, 16, 32], [24, 24, 24, 48], list(a.latt)]):
+    for i, latt in enumerate([] if a.only_point else [[16, 16, 16, 32], [24, 24, 24, 48], list(a.latt)]):
         G, u, L = _gauge(latt, a.eps, a.seed + 1 + i, a.t_bc, a.csw, a.kappa)
         del u
         handles.append(G)

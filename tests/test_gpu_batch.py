@@ -142,3 +142,27 @@ def test_invert12_point_propagator(q):
             got = P[..., :, s, :, c]
             assert np.linalg.norm(got - xo) / np.linalg.norm(xo) < 1e-8
     assert all(r["status"] == 1 for r in res)
+
+
+@pytest.mark.parametrize("tune", ["64,1,128,0", "128,1,256,0", "256,1,512,0", "64,2,256,0", "128,2,128,0",
+                                  "64,4,256,0", "128,4,512,0", "32,8,256,1", "32,8,128,2"])
+def test_batch_every_dslash_shape(q, tune, monkeypatch):
+    """Every block shape the autotuner can pick (sites per tile, rhs per
+    group, BLAS tile, tensor-core path) gives a converged, correct batch:
+    two lattices, a clover system, groups with partly filled slots."""
+    monkeypatch.setenv("QCU_BATCH_TUNE", tune)
+    systems = [_system(q, [8, 8, 8, 8], 21, 0.124, 5, False),
+               _system(q, [4, 4, 8, 8], 22, 0.125, 3, True)]
+    try:
+        res, got = q.invert_batch([(s["G"], s["x"], s["db"], s["kappa"], s["clover"]) for s in systems],
+                                  tol=1e-10, maxiter=4000, precision=32, gauge_precision=16, inner_iters=16,
+                                  inner_tol=0.1, gcr_k=4)
+        th, nr, bs, mma = [int(v) for v in tune.split(",")]
+        assert (got["dslash_threads"], got["dslash_rhs"], got["blas_sites"], got["mma"]) == (th, nr, bs, mma)
+        for r in res:
+            assert r["status"] == 1 and r["true_residual"] <= 1e-10, res
+        for s in systems:
+            _check(s, host(s["x"]), 1e-10)
+    finally:
+        for s in systems:
+            s["G"].close()

@@ -230,3 +230,25 @@ def test_invert_gcr_true_residual(q, prec, clover):
     r = b - O.mfull(host(x), U, latt, kappa, -1.0, True, A[0], A[1])
     assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05e-10
     assert info["reliable_updates"] >= 2  # outer steps
+
+
+def test_gauge_load_waits_for_inflight_copy(q):
+    """A gauge field still being copied host->device on another stream when
+    the handle is loaded: the load must see the finished field."""
+    import torch
+
+    latt = [16, 16, 16, 32]
+    U = O.gauge_smooth(latt, 0.25, 41)
+    psi = O.fermion_gauss(O.half_shape(latt), 42)
+    hU = torch.from_numpy(U).pin_memory()
+    dU = torch.zeros(U.shape, dtype=torch.complex128, device="cuda")
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        dU.copy_(hU, non_blocking=True)  # no synchronisation before the load
+        G = q.Gauge(dU, latt, t_boundary=-1.0)
+    try:
+        out = empty_like_dev(O.half_shape(latt))
+        G.dslash(out, dev(psi), 0)
+    finally:
+        G.close()
+    assert rel(host(out), O.dslash(psi, U, latt, 0, -1.0)) <= 1e-13
