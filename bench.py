@@ -390,25 +390,37 @@ def run_ours(args, world, rank, local, pg):
         dg = torch.empty_like(gauge)
         db = torch.empty_like(b)
         dx = torch.empty_like(b)
-        times = []
-        for i in range(2):
+        times, phases, all_phases = [], None, []
+        for i in range(3):
             torch.cuda.synchronize()
             s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
             s0.record()
             dg.copy_(hg, non_blocking=True)
             db.copy_(hb, non_blocking=True)
+            ev[0].record()
             with q.Gauge(dg, latt, t_boundary=T_BC) as G2:
+                ev[1].record()
                 info = G2.invert(dx, db, args.kappa, tol=TOL, maxiter=20000, **chosen_kw)
+                ev[2].record()
             hx.copy_(dx, non_blocking=True)
             s1.record()
             s1.synchronize()
             if info["status"] != 1:
                 raise RuntimeError(f"e2e solve failed: {info}")
             if i > 0:
-                times.append(s0.elapsed_time(s1) / 1e3)
+                t = s0.elapsed_time(s1) / 1e3
+                ph = {"total": round(t, 4), "h2d": round(s0.elapsed_time(ev[0]) / 1e3, 4),
+                      "gauge_load": round(ev[0].elapsed_time(ev[1]) / 1e3, 4),
+                      "solve": round(ev[1].elapsed_time(ev[2]) / 1e3, 4),
+                      "free_and_d2h": round(ev[2].elapsed_time(s1) / 1e3, 4), "iterations": info["iterations"]}
+                phases = ph if not times or t < min(times) else phases
+                all_phases.append(ph)
+                times.append(t)
         e2e_t = max_over_ranks(pg, min(times), dev)
         e2e = {"value": round(e2e_t, 4), "unit": "s", "h2d_bytes_per_step": hg.numel() * 16 + hb.numel() * 16,
-               "d2h_bytes_per_step": hx.numel() * 16}
+               "d2h_bytes_per_step": hx.numel() * 16, "samples_s": [round(t, 4) for t in times],
+               "phases": phases, "all_phases": all_phases}
 
     extra = {}
     if not args.no_extra and latt == LATT:

@@ -138,25 +138,15 @@ __device__ __forceinline__ void kb_dslash_tile(const BatchArgs &a, const int2 ti
         for (int c = 0; c < 12; c++) w[j][c] += x2[c] * (T)op.b2;
       }
       spinor_store<K, T>(bview<K>(d, op.out), s, w[j]);
-      if constexpr (RED == RED_DOT_RT) {
+      if constexpr (RED == RED_DOT_RT) {  // <rt, out>
         Cpx<T> rt[12];
         spinor_load<K, T>(bview<K>(d, op.rt), s, rt);
-#pragma unroll
-        for (int c = 0; c < 12; c++) {
-          red[j][0] += (double)rt[c].re * (double)w[j][c].re + (double)rt[c].im * (double)w[j][c].im;
-          red[j][1] += (double)rt[c].re * (double)w[j][c].im - (double)rt[c].im * (double)w[j][c].re;
-        }
-      } else if constexpr (RED == RED_TS_TT) {
-#pragma unroll
-        for (int c = 0; c < 12; c++) {
-          red[j][0] += (double)w[j][c].re * (double)x1[c].re + (double)w[j][c].im * (double)x1[c].im;
-          red[j][1] += (double)w[j][c].re * (double)x1[c].im - (double)w[j][c].im * (double)x1[c].re;
-          red[j][2] += (double)w[j][c].re * (double)w[j][c].re + (double)w[j][c].im * (double)w[j][c].im;
-        }
+        site_dot<T>(rt, w[j], red[j][0], red[j][1]);
+      } else if constexpr (RED == RED_TS_TT) {  // <out, x1>, |out|^2
+        site_dot<T>(w[j], x1, red[j][0], red[j][1]);
+        site_norm2<T>(w[j], red[j][2]);
       } else if constexpr (RED == RED_NORM) {
-#pragma unroll
-        for (int c = 0; c < 12; c++)
-          red[j][0] += (double)w[j][c].re * (double)w[j][c].re + (double)w[j][c].im * (double)w[j][c].im;
+        site_norm2<T>(w[j], red[j][0]);
       }
     }
   }
@@ -249,12 +239,8 @@ __device__ __forceinline__ void kb_xrupdate_tile(const BatchArgs &a, const int2 
     for (int c = 0; c < 12; c++) q[c] = q[c] - t[c] * w;
     spinor_store<K, T>(bview<K>(d, BV_R), s, q);
     spinor_load<K, T>(bview<K>(d, BV_RT), s, p);
-#pragma unroll
-    for (int c = 0; c < 12; c++) {
-      red[0] += (double)p[c].re * q[c].re + (double)p[c].im * q[c].im;
-      red[1] += (double)p[c].re * q[c].im - (double)p[c].im * q[c].re;
-      red[2] += (double)q[c].re * q[c].re + (double)q[c].im * q[c].im;
-    }
+    site_dot<T>(p, q, red[0], red[1]);
+    site_norm2<T>(q, red[2]);
   }
   batch_reduce<3, BB>(red, a, tile.x, tile.y, FIN_XR);
 }

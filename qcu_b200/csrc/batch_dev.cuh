@@ -22,15 +22,8 @@ __device__ __forceinline__ void batch_finish(const BatchArgs &a, int rhs, int op
   const int n = d.ntile[a.table];
   SolverState *st = a.st + rhs;
   __threadfence();
-  double acc[NV];
-#pragma unroll
-  for (int k = 0; k < NV; k++) acc[k] = 0.0;
-  for (int q = threadIdx.x; q < n; q += BS) {
-#pragma unroll
-    for (int k = 0; k < NV; k++) acc[k] += ((volatile const double *)P)[(size_t)q * RED_MAXV + k];
-  }
   double tot[NV];
-  block_sum<NV, BS>(acc, tot);
+  sum_partials<NV, BS>(P, n, tot);
   if (threadIdx.x == 0) {
     double s[RED_MAXV];
 #pragma unroll
@@ -41,14 +34,15 @@ __device__ __forceinline__ void batch_finish(const BatchArgs &a, int rhs, int op
   }
 }
 
-// partial of tile b of one rhs -> its partials; returns (to every thread of
+// partial of tile b of one rhs -> its partials (value k of tile b at
+// [k * ntile + b] in the rhs's region); returns (to every thread of
 // the block) whether this was the rhs's last tile.  `part` valid in thread 0.
 __device__ __forceinline__ bool batch_post(const BatchArgs &a, int rhs, int b, const double *part, int nv,
                                            bool *flag) {
   if (threadIdx.x == 0) {
     const RhsDesc &d = a.d[rhs];
-    double *P = a.partials + (size_t)d.poff[a.table] * RED_MAXV;
-    for (int k = 0; k < nv; k++) P[(size_t)b * RED_MAXV + k] = part[k];
+    double *P = a.partials + (size_t)d.poff[a.table] * RED_MAXV;  // this rhs's region, value-major
+    for (int k = 0; k < nv; k++) P[(size_t)k * d.ntile[a.table] + b] = part[k];
     __threadfence();
     const unsigned t = atomicAdd(&a.st[rhs].ticket, 1u);
     *flag = (t == (unsigned)d.ntile[a.table] - 1u);

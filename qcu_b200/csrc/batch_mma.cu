@@ -316,21 +316,13 @@ __device__ __forceinline__ void kb_dslash_mma_tile(const BatchArgs &a, const int
       for (int c = 0; c < 12; c++) w[c] += x1[c] * (float)op.b1;
     }
     spinor_store<SOA32, float>(bview<SOA32>(d, op.out), s, w);
-    if constexpr (RED == RED_DOT_RT) {
+    if constexpr (RED == RED_DOT_RT) {  // <rt, out>
       Cpx<float> rt[12];
       spinor_load<SOA32, float>(bview<SOA32>(d, op.rt), s, rt);
-#pragma unroll
-      for (int c = 0; c < 12; c++) {
-        red[0] += (double)rt[c].re * (double)w[c].re + (double)rt[c].im * (double)w[c].im;
-        red[1] += (double)rt[c].re * (double)w[c].im - (double)rt[c].im * (double)w[c].re;
-      }
-    } else if constexpr (RED == RED_TS_TT) {
-#pragma unroll
-      for (int c = 0; c < 12; c++) {
-        red[0] += (double)w[c].re * (double)x1[c].re + (double)w[c].im * (double)x1[c].im;
-        red[1] += (double)w[c].re * (double)x1[c].im - (double)w[c].im * (double)x1[c].re;
-        red[2] += (double)w[c].re * (double)w[c].re + (double)w[c].im * (double)w[c].im;
-      }
+      site_dot<float>(rt, w, red[0], red[1]);
+    } else if constexpr (RED == RED_TS_TT) {  // <out, x1>, |out|^2
+      site_dot<float>(w, x1, red[0], red[1]);
+      site_norm2<float>(w, red[2]);
     }
   }
   if constexpr (RED != RED_NONE) {
@@ -344,7 +336,7 @@ __device__ __forceinline__ void kb_dslash_mma_tile(const BatchArgs &a, const int
         const RhsDesc &d = a.d[grp.rhs[j]];
         double *P = a.partials + (size_t)d.poff[a.table] * RED_MAXV;
 #pragma unroll
-        for (int k = 0; k < NV; k++) P[(size_t)tile.y * RED_MAXV + k] = red[k];
+        for (int k = 0; k < NV; k++) P[(size_t)k * d.ntile[a.table] + tile.y] = red[k];
         __threadfence();
         const unsigned tk = atomicAdd(&a.st[grp.rhs[j]].ticket, 1u);
         last = (tk == (unsigned)d.ntile[a.table] - 1u);

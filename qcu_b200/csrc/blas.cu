@@ -89,12 +89,8 @@ __global__ void __launch_bounds__(BLAS_BLOCK) k_xrupdate(int Vh, VecSet vs, Solv
     for (int c = 0; c < 12; c++) q[c] = q[c] - t[c] * w;
     spinor_store<K, T>(sv<K>(vs.r, vs.rn, Vh), s, q);
     spinor_load<K, T>(sv<K>(vs.rt, vs.rtn, Vh), s, p);
-#pragma unroll
-    for (int c = 0; c < 12; c++) {
-      red[0] += (double)p[c].re * q[c].re + (double)p[c].im * q[c].im;
-      red[1] += (double)p[c].re * q[c].im - (double)p[c].im * q[c].re;
-      red[2] += (double)q[c].re * q[c].re + (double)q[c].im * q[c].im;
-    }
+    site_dot<T>(p, q, red[0], red[1]);
+    site_norm2<T>(q, red[2]);
   }
   grid_reduce<3, BLAS_BLOCK>(red, RedCtx{st, partials, FIN_XR});
 }
@@ -131,11 +127,7 @@ __global__ void __launch_bounds__(BLAS_BLOCK) k_rconv(int Vh, VecSet vs, SolverS
     spinor_load<SOA64, T>(sv<SOA64>(vs.r64, nullptr, Vh), s, r);
     if (K != SOA64 || vs.r != vs.r64) spinor_store<K, T>(sv<K>(vs.r, vs.rn, Vh), s, r);
     spinor_load<K, T>(sv<K>(vs.rt, vs.rtn, Vh), s, rt);
-#pragma unroll
-    for (int c = 0; c < 12; c++) {
-      red[0] += (double)rt[c].re * r[c].re + (double)rt[c].im * r[c].im;
-      red[1] += (double)rt[c].re * r[c].im - (double)rt[c].im * r[c].re;
-    }
+    site_dot<T>(rt, r, red[0], red[1]);
   }
   grid_reduce<2, BLAS_BLOCK>(red, RedCtx{st, partials, FIN_RCONV});
 }

@@ -10,6 +10,8 @@
 //     w   = A_p^{-1} w          (clover)       (qcu's give_clover, src/clover_dslash.cu:857-882)
 //     out = a*w + b1*x1 + b2*x2                (qcu's bistabcg_give_dest_o/_b__0, src/bistabcg.cu:73-96)
 //     and one of  <rt, out>,  <out, x1> & |out|^2,  |out|^2  reduced to the solver state.
+#include <algorithm>
+
 #include "internal.h"
 
 namespace qcu {
@@ -19,65 +21,70 @@ namespace qcu {
 // 3 blocks fit in 170 registers without spills
 #define DSLASH_MIN_BLOCKS(K) (((K) == AOS64 || (K) == SOA64) ? 3 : 1)
 
+// one output site: hop term, clover, epilogue, the site's share of the reduction
+template <int K, int G, int C, bool CLOV, int NX, int RED, int NV>
+__device__ __forceinline__ void dslash_site(const Geom &g, const DslashArgs &a, int s, double (&red)[NV]) {
+  using T = typename SpinorReal<K>::T;
+  Cpx<T> w[12];
+  const SpinorView<K> in{const_cast<void *>(a.in), const_cast<float *>(a.in_norm), g.Vh};
+  const GaugeView<G> U{a.gauge, G == GAOS64 ? g.Vh : pad_sites(g.Vh)};
+  wilson_hop_site<K, G, T>(w, in, U, g, s, a.parity, (T)a.t_bc);
+  if constexpr (CLOV) clover_apply_site<C, T>(CloverView<C>{a.clover, g.Vh}, s, w);
+  const T aa = (T)a.a;
+#pragma unroll
+  for (int c = 0; c < 12; c++) w[c] = w[c] * aa;
+  Cpx<T> x1[12];
+  if constexpr (NX >= 1) {
+    spinor_load<K, T>(SpinorView<K>{const_cast<void *>(a.x1), const_cast<float *>(a.x1_norm), g.Vh}, s, x1);
+    const T b1 = (T)a.b1;
+#pragma unroll
+    for (int c = 0; c < 12; c++) w[c] += x1[c] * b1;
+  }
+  if constexpr (NX >= 2) {
+    Cpx<T> x2[12];
+    spinor_load<K, T>(SpinorView<K>{const_cast<void *>(a.x2), const_cast<float *>(a.x2_norm), g.Vh}, s, x2);
+    const T b2 = (T)a.b2;
+#pragma unroll
+    for (int c = 0; c < 12; c++) w[c] += x2[c] * b2;
+  }
+  spinor_store<K, T>(SpinorView<K>{a.out, a.out_norm, g.Vh}, s, w);
+  if constexpr (RED == RED_DOT_RT) {  // <rt, out>
+    Cpx<T> rt[12];
+    spinor_load<K, T>(SpinorView<K>{const_cast<void *>(a.rt), const_cast<float *>(a.rt_norm), g.Vh}, s, rt);
+    site_dot<T>(rt, w, red[0], red[1]);
+  } else if constexpr (RED == RED_TS_TT) {  // <out, x1>, |out|^2
+    site_dot<T>(w, x1, red[0], red[1]);
+    site_norm2<T>(w, red[2]);
+  } else if constexpr (RED == RED_NORM) {
+    site_norm2<T>(w, red[0]);
+  }
+}
+
 template <int K, int G, int C, bool CLOV, int NX, int RED>
 __global__ void __launch_bounds__(DSLASH_BLOCK, DSLASH_MIN_BLOCKS(K)) k_dslash(Geom g, DslashArgs a, RedCtx rc) {
-  using T = typename SpinorReal<K>::T;
   if (!gate_open(rc.st, a.gate)) return;
   constexpr int NV = RED == RED_NONE ? 1 : (RED == RED_TS_TT ? 3 : (RED == RED_DOT_RT ? 2 : 1));
   double red[NV];
 #pragma unroll
   for (int k = 0; k < NV; k++) red[k] = 0.0;
-  const int s = blockIdx.x * DSLASH_BLOCK + threadIdx.x;
-  if (s < g.Vh) {
-    Cpx<T> w[12];
-    const SpinorView<K> in{const_cast<void *>(a.in), const_cast<float *>(a.in_norm), g.Vh};
-    const GaugeView<G> U{a.gauge, G == GAOS64 ? g.Vh : pad_sites(g.Vh)};
-    wilson_hop_site<K, G, T>(w, in, U, g, s, a.parity, (T)a.t_bc);
-    if constexpr (CLOV) clover_apply_site<C, T>(CloverView<C>{a.clover, g.Vh}, s, w);
-    const T aa = (T)a.a;
-#pragma unroll
-    for (int c = 0; c < 12; c++) w[c] = w[c] * aa;
-    Cpx<T> x1[12];
-    if constexpr (NX >= 1) {
-      spinor_load<K, T>(SpinorView<K>{const_cast<void *>(a.x1), const_cast<float *>(a.x1_norm), g.Vh}, s, x1);
-      const T b1 = (T)a.b1;
-#pragma unroll
-      for (int c = 0; c < 12; c++) w[c] += x1[c] * b1;
-    }
-    if constexpr (NX >= 2) {
-      Cpx<T> x2[12];
-      spinor_load<K, T>(SpinorView<K>{const_cast<void *>(a.x2), const_cast<float *>(a.x2_norm), g.Vh}, s, x2);
-      const T b2 = (T)a.b2;
-#pragma unroll
-      for (int c = 0; c < 12; c++) w[c] += x2[c] * b2;
-    }
-    spinor_store<K, T>(SpinorView<K>{a.out, a.out_norm, g.Vh}, s, w);
-    if constexpr (RED == RED_DOT_RT) {
-      Cpx<T> rt[12];
-      spinor_load<K, T>(SpinorView<K>{const_cast<void *>(a.rt), const_cast<float *>(a.rt_norm), g.Vh}, s, rt);
-#pragma unroll
-      for (int c = 0; c < 12; c++) {
-        red[0] += (double)rt[c].re * (double)w[c].re + (double)rt[c].im * (double)w[c].im;
-        red[1] += (double)rt[c].re * (double)w[c].im - (double)rt[c].im * (double)w[c].re;
-      }
-    } else if constexpr (RED == RED_TS_TT) {
-#pragma unroll
-      for (int c = 0; c < 12; c++) {
-        red[0] += (double)w[c].re * (double)x1[c].re + (double)w[c].im * (double)x1[c].im;
-        red[1] += (double)w[c].re * (double)x1[c].im - (double)w[c].im * (double)x1[c].re;
-        red[2] += (double)w[c].re * (double)w[c].re + (double)w[c].im * (double)w[c].im;
-      }
-    } else if constexpr (RED == RED_NORM) {
-#pragma unroll
-      for (int c = 0; c < 12; c++) red[0] += (double)w[c].re * (double)w[c].re + (double)w[c].im * (double)w[c].im;
-    }
+  if constexpr (RED == RED_NONE) {
+    const int s = blockIdx.x * DSLASH_BLOCK + threadIdx.x;  // one site per thread
+    if (s < g.Vh) dslash_site<K, G, C, CLOV, NX, RED, NV>(g, a, s, red);
+  } else {
+    // a grid of resident blocks strides over the sites, so the block
+    // reduction and the ticket (barriers, a fence, an atomic) are paid once
+    // per block rather than once per 128 sites
+    for (int s = blockIdx.x * DSLASH_BLOCK + threadIdx.x; s < g.Vh; s += gridDim.x * DSLASH_BLOCK)
+      dslash_site<K, G, C, CLOV, NX, RED, NV>(g, a, s, red);
+    grid_reduce<NV, DSLASH_BLOCK>(red, rc);
   }
-  if constexpr (RED != RED_NONE) grid_reduce<NV, DSLASH_BLOCK>(red, rc);
 }
 
 template <int K, int G, int C, bool CLOV, int NX, int RED>
 static void launch_t(const Geom &g, const DslashArgs &a, Context &ctx, cudaStream_t s) {
-  const int blocks = (g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK;
+  int blocks = (g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK;
+  // reductions: 3 resident blocks per SM (the reduction variants use 130-170 registers)
+  if (RED != RED_NONE) blocks = std::min(blocks, 3 * ctx.sms);
   RedCtx rc{ctx.st, ctx.partials, a.fin};
   if (RED != RED_NONE) {
     require(a.gate == GATE_ALWAYS || ctx.st != nullptr, "reduction without solver state");

@@ -51,7 +51,7 @@ Geom make_geom(const int latt[4]);  // validates: all > 0, Lx even
 
 constexpr int DSLASH_BLOCK = 128;
 constexpr int BLAS_BLOCK = 256;
-constexpr int MAX_REDUCE_BLOCKS = 148 * 16;
+constexpr int MAX_REDUCE_BLOCKS = 148 * 8;  // one resident wave of 256-thread blocks on B200
 
 inline int blas_grid(int n) {
   int g = (n + BLAS_BLOCK - 1) / BLAS_BLOCK;
@@ -100,6 +100,7 @@ struct Context {
   SolverState *st_host = nullptr;  // pinned mirror
   double *partials = nullptr;      // blocks * RED_MAXV doubles (grown to the largest grid used)
   size_t partials_blocks = 0;
+  int sms = 148;                   // multiprocessors of the device
   std::mutex mu;
   void ensure_partials(size_t blocks);
 };

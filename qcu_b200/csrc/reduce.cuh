@@ -157,11 +157,49 @@ __device__ inline void finalize(SolverState *st, int op, const double *s) {
   }
 }
 
+// Inner products of one site's 12 complex components.  The site's partial is
+// formed in the arithmetic type T of the storage (FP32 for FP32 and 16-bit
+// fields: 12 terms) and added to the FP64 accumulator once; sums across sites
+// (thread, block, grid) are FP64.  Converting every term to FP64 instead costs
+// ~100 FP64-pipe instructions per site, a third of an issue-bound kernel.
+template <typename T>
+__device__ __forceinline__ void site_dot(const Cpx<T> a[12], const Cpx<T> b[12], double &re, double &im) {
+  if constexpr (sizeof(T) == 8) {  // FP64 fields: every term straight into the accumulator
+#pragma unroll
+    for (int c = 0; c < 12; c++) {
+      re += a[c].re * b[c].re + a[c].im * b[c].im;
+      im += a[c].re * b[c].im - a[c].im * b[c].re;
+    }
+  } else {
+    T sr = 0, si = 0;
+#pragma unroll
+    for (int c = 0; c < 12; c++) {
+      sr += a[c].re * b[c].re + a[c].im * b[c].im;
+      si += a[c].re * b[c].im - a[c].im * b[c].re;
+    }
+    re += (double)sr;
+    im += (double)si;
+  }
+}
+template <typename T>
+__device__ __forceinline__ void site_norm2(const Cpx<T> a[12], double &n2) {
+  if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int c = 0; c < 12; c++) n2 += a[c].re * a[c].re + a[c].im * a[c].im;
+  } else {
+    T s = 0;
+#pragma unroll
+    for (int c = 0; c < 12; c++) s += a[c].re * a[c].re + a[c].im * a[c].im;
+    n2 += (double)s;
+  }
+}
+
 struct RedCtx {
   SolverState *st;
-  double *partials;  // [gridDim.x][RED_MAXV]
+  double *partials;  // value-major: value k of block b at [k * gridDim.x + b] (room for RED_MAXV values)
   int op;
 };
+
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -192,6 +230,23 @@ __device__ __forceinline__ void block_sum(double v[NV], double out[NV]) {
   __syncthreads();
 }
 
+// Sum of n partials (value-major, n per value) by the whole block, into
+// tot (valid in thread 0).  Plain L2 loads (the partials were written by
+// other blocks of this grid before their ticket), issued independently so
+// the block keeps many in flight; the order of the sum is fixed.
+template <int NV, int BS>
+__device__ __forceinline__ void sum_partials(const double *P, int n, double tot[NV]) {
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; k++) acc[k] = 0.0;
+#pragma unroll 4
+  for (int b = threadIdx.x; b < n; b += BS) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) acc[k] += __ldcg(P + (size_t)k * n + b);
+  }
+  block_sum<NV, BS>(acc, tot);
+}
+
 // Block partial -> global partials; the last block to arrive reduces all
 // partials in block order and runs the finalize op.
 template <int NV, int BS>
@@ -201,7 +256,7 @@ __device__ __forceinline__ void grid_reduce(double v[NV], const RedCtx &rc) {
   block_sum<NV, BS>(v, part);
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int k = 0; k < NV; k++) rc.partials[(size_t)blockIdx.x * RED_MAXV + k] = part[k];
+    for (int k = 0; k < NV; k++) rc.partials[(size_t)k * gridDim.x + blockIdx.x] = part[k];
     __threadfence();
     unsigned t = atomicAdd(&rc.st->ticket, 1u);
     last = (t == gridDim.x - 1);
@@ -209,15 +264,8 @@ __device__ __forceinline__ void grid_reduce(double v[NV], const RedCtx &rc) {
   __syncthreads();
   if (!last) return;
   __threadfence();
-  double acc[NV];
-#pragma unroll
-  for (int k = 0; k < NV; k++) acc[k] = 0.0;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) {
-#pragma unroll
-    for (int k = 0; k < NV; k++) acc[k] += ((volatile double *)rc.partials)[(size_t)b * RED_MAXV + k];
-  }
   double tot[NV];
-  block_sum<NV, BS>(acc, tot);
+  sum_partials<NV, BS>(rc.partials, (int)gridDim.x, tot);
   if (threadIdx.x == 0) {
     double s[RED_MAXV];
 #pragma unroll

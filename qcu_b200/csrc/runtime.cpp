@@ -109,6 +109,7 @@ Context &context() {
   auto c = std::make_unique<Context>();
   c->device = dev;
   QCU_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  QCU_CUDA(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev));
   QCU_CUDA(cudaMalloc(&c->st, sizeof(SolverState)));
   QCU_CUDA(cudaMemset(c->st, 0, sizeof(SolverState)));
   QCU_CUDA(cudaMallocHost(&c->st_host, sizeof(SolverState)));
