@@ -80,21 +80,25 @@ __device__ __forceinline__ void wilson_hop_group(Cpx<T> (&acc)[NR][12], const Sp
   hop_group<3, false>(acc, in, on, U, n, 1 - par, n, (t == 0) ? t_bc : T(1));
 }
 
-#define BDSL_MIN_BLOCKS(K, NT, NR) ((K) == SOA64 ? 384 / (NT) : ((NR) == 1 ? 1 : 1))
+// resident blocks asked of the register allocator: 4 x 128 threads (128
+// registers) for one FP32 rhs per thread, 3 x 128 for FP64; the
+// register-blocked groups keep their registers
+#define BDSL_MIN_BLOCKS(K, NT, NR) ((K) == SOA64 ? 384 / (NT) : ((NR) == 1 ? 512 / (NT) : 1))
 
 // Tile = (group of NR rhs of one system, block of NT sites); every thread
 // computes its site for all open rhs of the group, then the epilogue and the
 // per-rhs reductions rhs by rhs.
-template <int K, int G, bool CLOV, int NX, int RED, int NT, int NR>
-__device__ __forceinline__ void kb_dslash_tile(const BatchArgs &a, const int2 tile, BDslOp op) {
+template <int K, int G, bool CLOV, int NX, int RED, int NT, int NR, typename WR>
+__device__ __forceinline__ void kb_dslash_tile(const BatchArgs &a, const int2 tile, const BDslOp &op, WR &wr,
+                                               const BlockBatch &bb) {
   using T = Real<K>;
   constexpr int C = K == SOA64 ? CSOA64 : CSOA32;
-  const RhsGroup grp = a.groups[tile.x];
+  const RhsGroup &grp = bb.grp[tile.x];
   bool on[NR];
   bool any = false;
 #pragma unroll
   for (int j = 0; j < NR; j++) {
-    on[j] = j < grp.n && bgate(a, grp.rhs[j], op.gate);
+    on[j] = j < grp.n && bb.open[grp.rhs[j]];
     any = any || on[j];
   }
   if (!any) return;
@@ -153,7 +157,7 @@ __device__ __forceinline__ void kb_dslash_tile(const BatchArgs &a, const int2 ti
   if constexpr (RED != RED_NONE) {
 #pragma unroll
     for (int j = 0; j < NR; j++)
-      if (on[j]) batch_reduce<NV, NT>(red[j], a, grp.rhs[j], tile.y, op.fin);  // on[j] is uniform per block
+      if (on[j]) warp_red_add(wr, grp.rhs[j], red[j]);  // on[j] is uniform per block
   }
 }
 
@@ -166,9 +170,9 @@ constexpr int BB = 128;  // threads per BLAS tile
 
 // p = r + beta (p - omega v),  beta = (rho/rho_prev)(alpha/omega)
 template <int K>
-__device__ __forceinline__ void kb_pupdate_tile(const BatchArgs &a, const int2 tile) {
+__device__ __forceinline__ void kb_pupdate_tile(const BatchArgs &a, const int2 tile, const BlockBatch &bb) {
   using T = Real<K>;
-  if (!bgate(a, tile.x, BG_NOT_DONE)) return;
+  if (!bb.open[tile.x]) return;
   const RhsDesc &d = a.d[tile.x];
   SolverState *st = a.st + tile.x;
   const Cpx<double> rho(st->rho[0], st->rho[1]), rho_prev(st->rho_prev[0], st->rho_prev[1]),
@@ -193,9 +197,9 @@ __device__ __forceinline__ void kb_pupdate_tile(const BatchArgs &a, const int2 t
 
 // s = r - alpha v
 template <int K>
-__device__ __forceinline__ void kb_supdate_tile(const BatchArgs &a, const int2 tile) {
+__device__ __forceinline__ void kb_supdate_tile(const BatchArgs &a, const int2 tile, const BlockBatch &bb) {
   using T = Real<K>;
-  if (!bgate(a, tile.x, BG_NOT_DONE)) return;
+  if (!bb.open[tile.x]) return;
   const RhsDesc &d = a.d[tile.x];
   const SolverState *st = a.st + tile.x;
   const Cpx<T> al((T)st->alpha[0], (T)st->alpha[1]);
@@ -211,11 +215,11 @@ __device__ __forceinline__ void kb_supdate_tile(const BatchArgs &a, const int2 t
 }
 
 // x += alpha p + omega s ; r = s - omega t ; <rt, r>, |r|^2 -> FIN_XR
-template <int K, int XK>
-__device__ __forceinline__ void kb_xrupdate_tile(const BatchArgs &a, const int2 tile) {
+template <int K, int XK, typename WR>
+__device__ __forceinline__ void kb_xrupdate_tile(const BatchArgs &a, const int2 tile, WR &wr, const BlockBatch &bb) {
   using T = Real<K>;
   using TX = Real<XK>;
-  if (!bgate(a, tile.x, BG_NOT_DONE)) return;
+  if (!bb.open[tile.x]) return;
   const RhsDesc &d = a.d[tile.x];
   const SolverState *st = a.st + tile.x;
   const Cpx<T> w((T)st->omega[0], (T)st->omega[1]);
@@ -242,18 +246,18 @@ __device__ __forceinline__ void kb_xrupdate_tile(const BatchArgs &a, const int2 
     site_dot<T>(p, q, red[0], red[1]);
     site_norm2<T>(q, red[2]);
   }
-  batch_reduce<3, BB>(red, a, tile.x, tile.y, FIN_XR);
+  warp_red_add(wr, tile.x, red);
 }
 
 // r = rt = r64, p = v = x = 0 ; <rt, r>, |r64|^2 -> FIN_INIT.  An inactive
 // rhs reduces zeros, which FIN_INIT (inner mode) turns into "done".
-template <int K, int XK>
-__device__ __forceinline__ void kb_init_tile(const BatchArgs &a, const int2 tile) {
+template <int K, int XK, typename WR>
+__device__ __forceinline__ void kb_init_tile(const BatchArgs &a, const int2 tile, WR &wr, const BlockBatch &bb) {
   using T = Real<K>;
   using TX = Real<XK>;
   const RhsDesc &d = a.d[tile.x];
   double red[3] = {0, 0, 0};
-  if (a.active[tile.x]) {
+  if (bb.open[tile.x]) {
     BTILE_SITES(a, tile, d)
     for (int s = s_begin + threadIdx.x; s < s_end; s += BB) {
       Cpx<double> r64[12];
@@ -275,14 +279,14 @@ __device__ __forceinline__ void kb_init_tile(const BatchArgs &a, const int2 tile
       spinor_store<XK, TX>(bview<XK>(d, BV_X), s, zx);
     }
   }
-  batch_reduce<3, BB>(red, a, tile.x, tile.y, FIN_INIT);
+  warp_red_add(wr, tile.x, red);
 }
 
 // z = x in FP64 (active rhs)
 template <int XK>
-__device__ __forceinline__ void kb_xout_tile(const BatchArgs &a, const int2 tile) {
+__device__ __forceinline__ void kb_xout_tile(const BatchArgs &a, const int2 tile, const BlockBatch &bb) {
   using TX = Real<XK>;
-  if (!bgate(a, tile.x, BG_ACTIVE)) return;
+  if (!bb.open[tile.x]) return;
   const RhsDesc &d = a.d[tile.x];
   BTILE_SITES(a, tile, d)
   for (int s = s_begin + threadIdx.x; s < s_end; s += BB) {
@@ -332,8 +336,8 @@ __device__ __forceinline__ void st64(void *p, int s, const C v[12]) {
 }
 
 // sums[2j], sums[2j+1] = <W_j, w>, j < k
-__device__ __forceinline__ void kb_gcr_multidot_tile(const BatchArgs &a, const int2 tile, int k) {
-  if (!bgate(a, tile.x, BG_ACTIVE)) return;
+__device__ __forceinline__ void kb_gcr_multidot_tile(const BatchArgs &a, const int2 tile, int k, const BlockBatch &bb) {
+  if (!bb.open[tile.x]) return;
   const RhsDesc &d = a.d[tile.x];
   double red[2 * GCR_MAXK];
 #pragma unroll
@@ -359,8 +363,8 @@ __device__ __forceinline__ void kb_gcr_multidot_tile(const BatchArgs &a, const i
 }
 
 // W_k = w - sum beta_j W_j, Z_k = z - sum beta_j Z_j ; sums = |W_k|^2, <W_k, r>
-__device__ __forceinline__ void kb_gcr_orth_tile(const BatchArgs &a, const int2 tile, int k) {
-  if (!bgate(a, tile.x, BG_ACTIVE)) return;
+__device__ __forceinline__ void kb_gcr_orth_tile(const BatchArgs &a, const int2 tile, int k, const BlockBatch &bb) {
+  if (!bb.open[tile.x]) return;
   const RhsDesc &d = a.d[tile.x];
   const BatchCoef &cf = a.coef[tile.x];
   double red[3] = {0, 0, 0};
@@ -393,8 +397,8 @@ __device__ __forceinline__ void kb_gcr_orth_tile(const BatchArgs &a, const int2 
 }
 
 // x64 += alpha Z_k ; r64 -= alpha W_k ; sums[0] = |r64|^2
-__device__ __forceinline__ void kb_gcr_update_tile(const BatchArgs &a, const int2 tile, int k) {
-  if (!bgate(a, tile.x, BG_ACTIVE)) return;
+__device__ __forceinline__ void kb_gcr_update_tile(const BatchArgs &a, const int2 tile, int k, const BlockBatch &bb) {
+  if (!bb.open[tile.x]) return;
   const RhsDesc &d = a.d[tile.x];
   const C al(a.coef[tile.x].alpha[0], a.coef[tile.x].alpha[1]);
   double red[1] = {0};
@@ -423,44 +427,72 @@ __device__ __forceinline__ void kb_gcr_update_tile(const BatchArgs &a, const int
 // of a converged rhs costs a few instructions instead of a block launch.
 template <int K, int G, bool CLOV, int NX, int RED, int NT, int NR>
 __global__ void __launch_bounds__(NT, BDSL_MIN_BLOCKS(K, NT, NR)) kb_dslash(BatchArgs a, BDslOp op) {
-  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_dslash_tile<K, G, CLOV, NX, RED, NT, NR>(a, a.tiles[k], op);
+  constexpr int NV = RED == RED_NONE ? 1 : (RED == RED_TS_TT ? 3 : (RED == RED_DOT_RT ? 2 : 1));
+  __shared__ WarpRed<NV, NT / 32> wr;
+  __shared__ BlockBatch bb;
+  block_batch_init(a, bb, op.gate);
+  if constexpr (RED != RED_NONE) warp_red_zero(wr);
+  for_tiles(a, bb, [&](int2 tile) { kb_dslash_tile<K, G, CLOV, NX, RED, NT, NR>(a, tile, op, wr, bb); });
+  if constexpr (RED != RED_NONE) warp_red_post(a, wr, op.fin, op.gate);
 }
 
 template <int K>
 __global__ void __launch_bounds__(BB) kb_pupdate(BatchArgs a) {
-  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_pupdate_tile<K>(a, a.tiles[k]);
+  __shared__ BlockBatch bb;
+  block_batch_init(a, bb, BG_NOT_DONE);
+  for_tiles(a, bb, [&](int2 tile) { kb_pupdate_tile<K>(a, tile, bb); });
 }
 
 template <int K>
 __global__ void __launch_bounds__(BB) kb_supdate(BatchArgs a) {
-  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_supdate_tile<K>(a, a.tiles[k]);
+  __shared__ BlockBatch bb;
+  block_batch_init(a, bb, BG_NOT_DONE);
+  for_tiles(a, bb, [&](int2 tile) { kb_supdate_tile<K>(a, tile, bb); });
 }
 
 template <int K, int XK>
 __global__ void __launch_bounds__(BB) kb_xrupdate(BatchArgs a) {
-  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_xrupdate_tile<K, XK>(a, a.tiles[k]);
+  __shared__ WarpRed<3, BB / 32> wr;
+  __shared__ BlockBatch bb;
+  block_batch_init(a, bb, BG_NOT_DONE);
+  warp_red_zero(wr);
+  for_tiles(a, bb, [&](int2 tile) { kb_xrupdate_tile<K, XK>(a, tile, wr, bb); });
+  warp_red_post(a, wr, FIN_XR, BG_NOT_DONE);
 }
 
 template <int K, int XK>
 __global__ void __launch_bounds__(BB) kb_init(BatchArgs a) {
-  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_init_tile<K, XK>(a, a.tiles[k]);
+  __shared__ WarpRed<3, BB / 32> wr;
+  __shared__ BlockBatch bb;
+  block_batch_init(a, bb, BG_ACTIVE);
+  warp_red_zero(wr);
+  for_tiles(a, bb, [&](int2 tile) { kb_init_tile<K, XK>(a, tile, wr, bb); });
+  warp_red_post(a, wr, FIN_INIT, BG_ALWAYS);  // inactive rhs reduce zeros: FIN_INIT marks them done
 }
 
 template <int XK>
 __global__ void __launch_bounds__(BB) kb_xout(BatchArgs a) {
-  for (int k = blockIdx.x; k < a.ntiles; k += gridDim.x) kb_xout_tile<XK>(a, a.tiles[k]);
+  __shared__ BlockBatch bb;
+  block_batch_init(a, bb, BG_ACTIVE);
+  for_tiles(a, bb, [&](int2 tile) { kb_xout_tile<XK>(a, tile, bb); });
 }
 
 __global__ void __launch_bounds__(BB) kb_gcr_multidot(BatchArgs a, int k) {
-  for (int q = blockIdx.x; q < a.ntiles; q += gridDim.x) kb_gcr_multidot_tile(a, a.tiles[q], k);
+  __shared__ BlockBatch bb;
+  block_batch_init(a, bb, BG_ACTIVE);
+  for_tiles(a, bb, [&](int2 tile) { kb_gcr_multidot_tile(a, tile, k, bb); });
 }
 
 __global__ void __launch_bounds__(BB) kb_gcr_orth(BatchArgs a, int k) {
-  for (int q = blockIdx.x; q < a.ntiles; q += gridDim.x) kb_gcr_orth_tile(a, a.tiles[q], k);
+  __shared__ BlockBatch bb;
+  block_batch_init(a, bb, BG_ACTIVE);
+  for_tiles(a, bb, [&](int2 tile) { kb_gcr_orth_tile(a, tile, k, bb); });
 }
 
 __global__ void __launch_bounds__(BB) kb_gcr_update(BatchArgs a, int k) {
-  for (int q = blockIdx.x; q < a.ntiles; q += gridDim.x) kb_gcr_update_tile(a, a.tiles[q], k);
+  __shared__ BlockBatch bb;
+  block_batch_init(a, bb, BG_ACTIVE);
+  for_tiles(a, bb, [&](int2 tile) { kb_gcr_update_tile(a, tile, k, bb); });
 }
 
 // ---------------------------------------------------------------- launchers
@@ -468,13 +500,19 @@ __global__ void __launch_bounds__(BB) kb_gcr_update(BatchArgs a, int k) {
 // thread count (or fewer when the table has fewer tiles); each block then
 // walks the tile table with a stride of the grid.
 static int persistent_grid(const BatchArgs &a, int threads) {
-  const int cap = std::max(1, a.sms) * std::max(1, 2048 / threads);
+  const int cap = std::min(BATCH_POST_GRID, std::max(1, a.sms) * std::max(1, 1024 / threads));
+  return std::max(1, std::min(a.ntiles, cap));
+}
+// the hopping kernels: the blocks their registers let reside per SM
+static int dslash_grid(const BatchArgs &a, int per_sm) {
+  const int cap = std::min(BATCH_POST_GRID, std::max(1, a.sms) * std::max(1, per_sm));
   return std::max(1, std::min(a.ntiles, cap));
 }
 template <int K, int G, bool CLOV, int NT, int NR>
 static void bdsl_nx(const BatchArgs &a, const BDslOp &op, cudaStream_t s) {
   const int nx = op.x2 >= 0 ? 2 : (op.x1 >= 0 ? 1 : 0);
-#define QCU_BD(NX, RED) kb_dslash<K, G, CLOV, NX, RED, NT, NR><<<persistent_grid(a, NT), NT, 0, s>>>(a, op)
+  constexpr int per_sm = (K != SOA64 && NR == 1) ? 512 / NT : 384 / NT;
+#define QCU_BD(NX, RED) kb_dslash<K, G, CLOV, NX, RED, NT, NR><<<dslash_grid(a, per_sm), NT, 0, s>>>(a, op)
   // the combinations the batched solver uses: inner (0,-), (1,<rt,v>), (1,<t,s>|t|^2);
   // FP64 outer (0,-), (1,-), (2,|r|^2)
   if (nx == 0 && op.red == RED_NONE) {

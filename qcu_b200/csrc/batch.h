@@ -19,6 +19,7 @@ namespace qcu {
 
 constexpr int BATCH_MAX_RHS = 64;
 constexpr int BATCH_MAX_NR = 8;  // right-hand sides per dslash group
+constexpr int BATCH_POST_GRID = 148 * 8;  // largest grid of a kernel that reduces once per block
 
 // right-hand sides of one system that the dslash advances together: one
 // thread per site computes all of them, decoding each link once
@@ -62,6 +63,7 @@ struct BatchArgs {
   const RhsDesc *d = nullptr;     // [nrhs]
   const int2 *tiles = nullptr;    // [ntiles] (rhs, block); dslash tables: (group, block)
   const RhsGroup *groups = nullptr;  // dslash tables: the groups tiles refer to
+  int ngroups = 0;
   SolverState *st = nullptr;      // [nrhs]
   double *partials = nullptr;     // [tiles of the finest table][RED_MAXV]
   const int *active = nullptr;    // [nrhs]

@@ -173,7 +173,6 @@ struct MmaSmem {
     float2 out[8][MMA_SITES][12];
   };
   int n[8][MMA_SITES];
-  bool last[8];
 };
 
 // stage hop H: warp w = rhs slot w, lane = site; projected half spinors to smem
@@ -206,15 +205,15 @@ __device__ __forceinline__ void hop_step(MmaSmem &sm, float (&d1)[4][4], float (
   __syncthreads();
 }
 
-template <int G, bool CLOV, int NX, int RED, int SPLIT>
+template <int G, bool CLOV, int NX, int RED, int SPLIT, typename WR>
 __device__ __forceinline__ void kb_dslash_mma_tile(const BatchArgs &a, const int2 tile, const BDslOp &op,
-                                                   MmaSmem &sm) {
-  const RhsGroup grp = a.groups[tile.x];
+                                                   MmaSmem &sm, WR &wr, const BlockBatch &bb) {
+  const RhsGroup &grp = bb.grp[tile.x];
   bool on[8];
   bool any = false;
 #pragma unroll
   for (int j = 0; j < 8; j++) {
-    on[j] = j < grp.n && bgate(a, grp.rhs[j], op.gate);
+    on[j] = j < grp.n && bb.open[grp.rhs[j]];
     any = any || on[j];
   }
   if (!any) return;
@@ -326,41 +325,28 @@ __device__ __forceinline__ void kb_dslash_mma_tile(const BatchArgs &a, const int
     }
   }
   if constexpr (RED != RED_NONE) {
-    // per-rhs partial of this tile from warp j; the whole block then finishes
-    // every rhs whose last tile this was, one after another
-#pragma unroll
-    for (int k = 0; k < NV; k++) red[k] = warp_sum(red[k]);
-    if (lane == 0) {
-      bool last = false;
-      if (on_j) {
-        const RhsDesc &d = a.d[grp.rhs[j]];
-        double *P = a.partials + (size_t)d.poff[a.table] * RED_MAXV;
-#pragma unroll
-        for (int k = 0; k < NV; k++) P[(size_t)k * d.ntile[a.table] + tile.y] = red[k];
-        __threadfence();
-        const unsigned tk = atomicAdd(&a.st[grp.rhs[j]].ticket, 1u);
-        last = (tk == (unsigned)d.ntile[a.table] - 1u);
-      }
-      sm.last[j] = last;
-    }
-    __syncthreads();
-    for (int jj = 0; jj < 8; jj++) {
-      if (sm.last[jj]) batch_finish<NV, MMA_THREADS>(a, grp.rhs[jj], op.fin);  // uniform: shared flag
-    }
+    if (on_j) warp_red_add(wr, grp.rhs[j], red);  // warp j's share of rhs slot j
   }
   __syncthreads();  // the next tile overwrites the shared memory the epilogue read
 }
 
 template <int G, bool CLOV, int NX, int RED, int SPLIT>
 __global__ void __launch_bounds__(MMA_THREADS) kb_dslash_mma(BatchArgs a, BDslOp op) {
+  constexpr int NV = RED == RED_NONE ? 1 : (RED == RED_TS_TT ? 3 : (RED == RED_DOT_RT ? 2 : 1));
   __shared__ MmaSmem sm;
-  for (int q = blockIdx.x; q < a.ntiles; q += gridDim.x) kb_dslash_mma_tile<G, CLOV, NX, RED, SPLIT>(a, a.tiles[q], op, sm);
+  __shared__ WarpRed<NV, MMA_THREADS / 32> wr;
+  __shared__ BlockBatch bb;
+  block_batch_init(a, bb, op.gate);
+  if constexpr (RED != RED_NONE) warp_red_zero(wr);
+  for_tiles(a, bb, [&](int2 tile) { kb_dslash_mma_tile<G, CLOV, NX, RED, SPLIT>(a, tile, op, sm, wr, bb); });
+  if constexpr (RED != RED_NONE) warp_red_post(a, wr, op.fin, op.gate);
 }
 
 template <int G, bool CLOV, int SPLIT>
 static void mma_nx(const BatchArgs &a, const BDslOp &op, cudaStream_t s) {
   const int nx = op.x2 >= 0 ? 2 : (op.x1 >= 0 ? 1 : 0);
-  const dim3 grid(std::max(1, std::min(a.ntiles, std::max(1, a.sms) * 3))), block(MMA_THREADS);  // 3 resident per SM
+  const dim3 grid(std::max(1, std::min(a.ntiles, std::min(BATCH_POST_GRID, std::max(1, a.sms) * 2)))),
+      block(MMA_THREADS);  // 2 resident per SM
   if (nx == 0 && op.red == RED_NONE) kb_dslash_mma<G, CLOV, 0, RED_NONE, SPLIT><<<grid, block, 0, s>>>(a, op);
   else if (nx == 1 && op.red == RED_DOT_RT) kb_dslash_mma<G, CLOV, 1, RED_DOT_RT, SPLIT><<<grid, block, 0, s>>>(a, op);
   else if (nx == 1 && op.red == RED_TS_TT) kb_dslash_mma<G, CLOV, 1, RED_TS_TT, SPLIT><<<grid, block, 0, s>>>(a, op);

@@ -172,7 +172,7 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
   // partials: enough for the finest table any candidate uses (32 sites per tile)
   size_t max_tiles = 0;
   for (int r = 0; r < R; r++) max_tiles += (Vh[r] + 31) / 32;
-  c.partials.ensure(max_tiles * RED_MAXV * sizeof(double));
+  c.partials.ensure(std::max(max_tiles, (size_t)R * BATCH_POST_GRID) * RED_MAXV * sizeof(double));
   c.st.ensure(sizeof(SolverState) * BATCH_MAX_RHS);
   c.active.ensure(sizeof(int) * BATCH_MAX_RHS);
   c.coef.ensure(sizeof(BatchCoef) * BATCH_MAX_RHS);
@@ -242,6 +242,7 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
         QCU_CUDA(cudaMemcpyAsync(gb.p, grp[t]->data(), sizeof(RhsGroup) * grp[t]->size(), cudaMemcpyHostToDevice,
                                  st));
         a.groups = gb.as<RhsGroup>();
+        a.ngroups = (int)grp[t]->size();
       }
       a.st = c.st.as<SolverState>();
       a.partials = c.partials.as<double>();
