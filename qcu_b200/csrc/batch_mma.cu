@@ -115,19 +115,19 @@ __device__ __forceinline__ void project(const Cpx<float> (&psi)[12], Cpx<float> 
 // the 8 rhs (lane g = rhs slot, lane t = k column), B from the staged link.
 // SPLIT 3: 3xTF32 (FP32-accurate); 1: one TF32 product.
 template <int H, int SPLIT>
-__device__ __forceinline__ void mma_hop(float (&d1)[4], float (&d2)[4], const float2 (*hs)[6], const float2 *u, int g,
-                                        int t) {
+__device__ __forceinline__ void mma_hop(float (&d1)[4], float (&d2)[4], const float2 (*hs)[6][MMA_SITES + 1], int sl,
+                                        const float2 *u, int g, int t) {
   constexpr int MU = H >> 1;
   constexpr int S = (H & 1) == 0 ? -1 : 1;
   const int c1 = t >> 1, pt = t & 1;
   const bool has2 = t < 2;  // column t + 4 is colour 2 for t < 2, padding otherwise
-  const float2 *h = hs[g];
+  const float2 (*h)[MMA_SITES + 1] = hs[g];  // [component][site] of rhs slot g
   auto cx = [](float2 v) { return Cpx<float>(v.x, v.y); };
   Cpx<float> h1[2], h2[2];  // half spins k = 0, 1 at colours c1 and 2
-  h1[0] = cx(h[c1]);
-  h1[1] = cx(h[3 + c1]);
-  h2[0] = has2 ? cx(h[2]) : Cpx<float>(0, 0);
-  h2[1] = has2 ? cx(h[5]) : Cpx<float>(0, 0);
+  h1[0] = cx(h[c1][sl]);
+  h1[1] = cx(h[3 + c1][sl]);
+  h2[0] = has2 ? cx(h[2][sl]) : Cpx<float>(0, 0);
+  h2[1] = has2 ? cx(h[5][sl]) : Cpx<float>(0, 0);
   // lower spins: s g_m h_gcol(m)
   const Cpx<float> l1_2 = unit_mul<S * gre(MU, 2), S * gim(MU, 2)>(h1[gcol(MU, 2)]);
   const Cpx<float> l1_3 = unit_mul<S * gre(MU, 3), S * gim(MU, 3)>(h1[gcol(MU, 3)]);
@@ -168,7 +168,7 @@ struct MmaSmem {
   union {
     struct {
       float2 u[8][MMA_SITES][9];
-      float2 h[MMA_SITES][8][6];
+      float2 h[8][6][MMA_SITES + 1];  // [rhs slot][component][site]: padded against bank conflicts
     } in;
     float2 out[8][MMA_SITES][12];
   };
@@ -188,7 +188,7 @@ __device__ __forceinline__ void stage_hop(MmaSmem &sm, const float4 *in, bool li
     for (int k = 0; k < 6; k++) h[k] = Cpx<float>(0, 0);
   }
 #pragma unroll
-  for (int k = 0; k < 6; k++) sm.in.h[lane][slot][k] = make_float2(h[k].re, h[k].im);
+  for (int k = 0; k < 6; k++) sm.in.h[slot][k][lane] = make_float2(h[k].re, h[k].im);
 }
 
 template <int H, int SPLIT>
@@ -200,7 +200,7 @@ __device__ __forceinline__ void hop_step(MmaSmem &sm, float (&d1)[4][4], float (
 #pragma unroll
   for (int q = 0; q < MMA_SITES / 8; q++) {
     const int sl = warp * (MMA_SITES / 8) + q;
-    if (s0 + sl < Vh) mma_hop<H, SPLIT>(d1[q], d2[q], sm.in.h[sl], sm.in.u[H][sl], gq, t);  // warp-uniform
+    if (s0 + sl < Vh) mma_hop<H, SPLIT>(d1[q], d2[q], sm.in.h, sl, sm.in.u[H][sl], gq, t);  // warp-uniform
   }
   __syncthreads();
 }

@@ -18,8 +18,10 @@ namespace qcu {
 
 // resident blocks per SM requested from the register allocator: the FP64
 // kernels would otherwise take ~176 registers (2 blocks of 128 threads per SM);
-// 3 blocks fit in 170 registers without spills
-#define DSLASH_MIN_BLOCKS(K) (((K) == AOS64 || (K) == SOA64) ? 3 : 1)
+// 3 blocks fit in 170 registers without spills.  The 16/32-bit variants with a
+// reduction stride over the sites with one resident wave of 4 blocks per SM
+// (128 registers).
+#define DSLASH_MIN_BLOCKS(K, RED) (((K) == AOS64 || (K) == SOA64) ? 3 : ((RED) == RED_NONE ? 1 : 4))
 
 // one output site: hop term, clover, epilogue, the site's share of the reduction
 template <int K, int G, int C, bool CLOV, int NX, int RED, int NV>
@@ -61,7 +63,7 @@ __device__ __forceinline__ void dslash_site(const Geom &g, const DslashArgs &a, 
 }
 
 template <int K, int G, int C, bool CLOV, int NX, int RED>
-__global__ void __launch_bounds__(DSLASH_BLOCK, DSLASH_MIN_BLOCKS(K)) k_dslash(Geom g, DslashArgs a, RedCtx rc) {
+__global__ void __launch_bounds__(DSLASH_BLOCK, DSLASH_MIN_BLOCKS(K, RED)) k_dslash(Geom g, DslashArgs a, RedCtx rc) {
   if (!gate_open(rc.st, a.gate)) return;
   constexpr int NV = RED == RED_NONE ? 1 : (RED == RED_TS_TT ? 3 : (RED == RED_DOT_RT ? 2 : 1));
   double red[NV];
@@ -83,8 +85,8 @@ __global__ void __launch_bounds__(DSLASH_BLOCK, DSLASH_MIN_BLOCKS(K)) k_dslash(G
 template <int K, int G, int C, bool CLOV, int NX, int RED>
 static void launch_t(const Geom &g, const DslashArgs &a, Context &ctx, cudaStream_t s) {
   int blocks = (g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK;
-  // reductions: 3 resident blocks per SM (the reduction variants use 130-170 registers)
-  if (RED != RED_NONE) blocks = std::min(blocks, 3 * ctx.sms);
+  // reductions: one resident wave (128 registers for 16/32-bit fields: 4 blocks per SM; FP64: 3)
+  if (RED != RED_NONE) blocks = std::min(blocks, DSLASH_MIN_BLOCKS(K, RED) * ctx.sms);
   RedCtx rc{ctx.st, ctx.partials, a.fin};
   if (RED != RED_NONE) {
     require(a.gate == GATE_ALWAYS || ctx.st != nullptr, "reduction without solver state");

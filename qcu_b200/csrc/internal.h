@@ -66,6 +66,7 @@ size_t spinor_norm_bytes(int kind, int Vh);
 struct DevBuf {
   void *p = nullptr;
   size_t n = 0;
+  cudaStream_t stream = nullptr;  // the context stream the buffer was allocated on (and is freed on)
   DevBuf() = default;
   DevBuf(const DevBuf &) = delete;
   DevBuf &operator=(const DevBuf &) = delete;

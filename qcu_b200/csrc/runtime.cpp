@@ -67,9 +67,32 @@ size_t spinor_bytes(int kind, int Vh) {
 size_t spinor_norm_bytes(int kind, int Vh) { return kind == SOA16 ? (size_t)pad_sites(Vh) * 4 : 0; }
 
 // ---------------------------------------------------------------- buffers
+// Device buffers come from a memory pool of the library's own, ordered on the
+// context stream, that keeps freed memory for reuse (release threshold: never).
+// A gauge handle loaded and freed per solve then costs no cudaMalloc/cudaFree,
+// whose page mapping on multi-GB buffers took 10-300 ms per call on B200.
+static std::mutex g_pool_mu;
+static std::map<int, cudaMemPool_t> g_pools;
+
+static cudaMemPool_t pool_for(int dev) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto it = g_pools.find(dev);
+  if (it != g_pools.end()) return it->second;
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool;
+  QCU_CUDA(cudaMemPoolCreate(&pool, &props));
+  uint64_t keep = UINT64_MAX;
+  QCU_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  g_pools[dev] = pool;
+  return pool;
+}
+
 DevBuf::~DevBuf() { release(); }
 void DevBuf::release() {
-  if (p) cudaFree(p);
+  if (p) cudaFreeAsync(p, stream);
   p = nullptr;
   n = 0;
 }
@@ -77,7 +100,9 @@ void DevBuf::ensure(size_t bytes) {
   if (bytes <= n) return;
   release();
   if (bytes == 0) return;
-  QCU_CUDA(cudaMalloc(&p, bytes));
+  Context &ctx = context();
+  stream = ctx.stream;
+  QCU_CUDA(cudaMallocFromPoolAsync(&p, bytes, pool_for(ctx.device), stream));
   n = bytes;
 }
 
