@@ -352,6 +352,48 @@ def point_sources(latt, origin, device="cuda"):
     return b
 
 
+def wall_source(latt, t: int, spin: int, color: int, device="cuda"):
+    """Wall source at time slice t: 1 on every site of the slice for (spin,
+    color), PyQuda layout [2, Lt, Lz, Ly, Lx/2, 4, 3]
+    (python/PyQuda/pyquda/utils/source.py:25-34)."""
+    import torch
+
+    L = Layout(tuple(latt))
+    b = torch.zeros(L.full, dtype=torch.complex128, device=device)
+    b[:, t, :, :, :, spin, color] = 1.0
+    return b
+
+
+def momentum_phase(latt, mom, device="cuda"):
+    """exp(i 2 pi sum_k p_k x_k / L_k) on the spatial coordinates, PyQuda
+    even-odd layout [2, Lt, Lz, Ly, Lx/2]."""
+    import math
+
+    import torch
+
+    Lx, Ly, Lz, Lt = [int(v) for v in latt]
+    t, z, y, xh = torch.meshgrid(torch.arange(Lt), torch.arange(Lz), torch.arange(Ly), torch.arange(Lx // 2),
+                                 indexing="ij")
+    out = torch.empty((2, Lt, Lz, Ly, Lx // 2), dtype=torch.complex128)
+    px, py, pz = [float(v) for v in mom]
+    for p in (0, 1):
+        x = (2 * xh + ((t + z + y + p) % 2)).to(torch.float64)
+        arg = 2 * math.pi * (px * x / Lx + py * y.to(torch.float64) / Ly + pz * z.to(torch.float64) / Lz)
+        out[p] = torch.polar(torch.ones_like(arg), arg)
+    return out.to(device)
+
+
+def momentum_source(latt, t: int, phase, spin: int, color: int, device="cuda"):
+    """Momentum (wall) source: the phase on time slice t for (spin, color)
+    (python/PyQuda/pyquda/utils/source.py:37-46)."""
+    import torch
+
+    L = Layout(tuple(latt))
+    b = torch.zeros(L.full, dtype=torch.complex128, device=device)
+    b[:, t, :, :, :, spin, color] = phase.to(device)[:, t]
+    return b
+
+
 def invert12(G: "Gauge", kappa: float, origin, clover: bool = False, **kw):
     """Propagator from a point source at `origin`: the 12 spin-colour solves in
     one batched solve.  Returns (propagator [2, Lt, Lz, Ly, Lx/2, 4, 4, 3, 3] =
