@@ -18,10 +18,12 @@ namespace qcu {
 
 // resident blocks per SM requested from the register allocator: the FP64
 // kernels would otherwise take ~176 registers (2 blocks of 128 threads per SM);
-// 3 blocks fit in 170 registers without spills.  The 16/32-bit variants with a
-// reduction stride over the sites with one resident wave of 4 blocks per SM
-// (128 registers).
-#define DSLASH_MIN_BLOCKS(K, RED) (((K) == AOS64 || (K) == SOA64) ? 3 : ((RED) == RED_NONE ? 1 : 4))
+// 3 blocks fit in 170 registers without spills.  The variants with a reduction
+// stride over the sites with one resident wave of 3 blocks per SM (forcing the
+// 16/32-bit ones to 128 registers for a 4th block measured slower).
+#define DSLASH_MIN_BLOCKS(K, RED) (((K) == AOS64 || (K) == SOA64) ? 3 : 1)
+// resident blocks per SM of the reducing variants (grid of the strided launch)
+#define DSLASH_RED_BLOCKS_PER_SM 3
 
 // one output site: hop term, clover, epilogue, the site's share of the reduction
 template <int K, int G, int C, bool CLOV, int NX, int RED, int NV>
@@ -85,8 +87,8 @@ __global__ void __launch_bounds__(DSLASH_BLOCK, DSLASH_MIN_BLOCKS(K, RED)) k_dsl
 template <int K, int G, int C, bool CLOV, int NX, int RED>
 static void launch_t(const Geom &g, const DslashArgs &a, Context &ctx, cudaStream_t s) {
   int blocks = (g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK;
-  // reductions: one resident wave (128 registers for 16/32-bit fields: 4 blocks per SM; FP64: 3)
-  if (RED != RED_NONE) blocks = std::min(blocks, DSLASH_MIN_BLOCKS(K, RED) * ctx.sms);
+  // reductions: one resident wave (the 16/32-bit reducing variants take ~167 registers, FP64 170)
+  if (RED != RED_NONE) blocks = std::min(blocks, DSLASH_RED_BLOCKS_PER_SM * ctx.sms);
   RedCtx rc{ctx.st, ctx.partials, a.fin};
   if (RED != RED_NONE) {
     require(a.gate == GATE_ALWAYS || ctx.st != nullptr, "reduction without solver state");
