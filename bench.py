@@ -165,6 +165,102 @@ def cpu_sample(latt, kappa, gauge_np, b_np, plain_iters, budget_s=12.0):
             "seconds_per_iteration": per_iter}
 
 
+def cpu_dslash_medians(latt):
+    """Median time of one FP64 hopping-term application of the CPU oracle on
+    8^4 and on `latt`, with 1 host thread and with all of them."""
+    import numpy as np
+
+    import oracle as O
+
+    out = {}
+    nthreads = O.get_threads()
+    for lt in ([8, 8, 8, 8], list(latt)):
+        U = O.gauge_smooth(lt, EPS, GAUGE_SEED)
+        psi = O.fermion_gauss(O.half_shape(lt), SRC_SEED)
+        rec = {}
+        for th in (1, nthreads):
+            O.set_threads(th)
+            O.dslash(psi, U, lt, 0, T_BC)
+            ts = []
+            for _ in range(3 if lt[3] >= 32 else 9):
+                t0 = time.perf_counter()
+                O.dslash(psi, U, lt, 0, T_BC)
+                ts.append(time.perf_counter() - t0)
+            rec[f"threads_{th}"] = round(1e3 * float(np.median(ts)), 3)
+        out["x".join(map(str, lt))] = rec
+    O.set_threads(nthreads)
+    return {"unit": "ms per application (FP64, one parity)", **out}
+
+
+def reference_gpu(latt):
+    """qcu's own CUDA code, built from its sources for sm_100a
+    (oracle/_ref/libqcu_ref.so), on this GPU: the full dslashQcu call
+    (including qcu's per-call setup and in-place layout permutations) at
+    `latt`, and ncclBistabCgQcu (its fixed kappa 0.125 and absolute 1e-9
+    criterion) on 16^3 x 32.  qcu prints a line per dslash; its output is
+    kept off this process's stdout.  None when the build or a GPU is absent."""
+    import ctypes
+
+    path = os.path.join(ROOT, "oracle", "_ref", "libqcu_ref.so")
+    try:
+        import torch
+
+        if not (os.path.exists(path) and torch.cuda.is_available()):
+            return None
+        import qcu_b200 as q
+
+        ref = ctypes.CDLL(path)
+        Pp, vp = ctypes.POINTER(q.QcuParam), ctypes.c_void_p
+        ref.dslashQcu.argtypes = [vp, vp, vp, Pp, ctypes.c_int]
+        ref.dslashQcu.restype = None
+        ref.ncclBistabCgQcu.argtypes = [vp, vp, vp, Pp, Pp]
+        ref.ncclBistabCgQcu.restype = None
+        sys.stdout.flush()
+        saved = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+        try:
+            out = {}
+            L = q.Layout(tuple(latt))
+            U = torch.empty(L.gauge, dtype=torch.complex128, device="cuda")
+            q.gauge_random(U, latt, 1, EPS, GAUGE_SEED)
+            psi = torch.empty(L.half, dtype=torch.complex128, device="cuda")
+            q.fermion_random(psi, psi.numel(), 0, SRC_SEED)
+            o = torch.empty_like(psi)
+            par = q.QcuParam(latt)
+            ref.dslashQcu(o.data_ptr(), psi.data_ptr(), U.data_ptr(), ctypes.byref(par), 0)
+            ts = []
+            for _ in range(3):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                ref.dslashQcu(o.data_ptr(), psi.data_ptr(), U.data_ptr(), ctypes.byref(par), 0)
+                torch.cuda.synchronize()
+                ts.append(time.perf_counter() - t0)
+            out["dslashQcu_call_ms_" + "x".join(map(str, latt))] = round(1e3 * min(ts), 2)
+            del U, psi, o
+            small = [16, 16, 16, 32]
+            Ls = q.Layout(tuple(small))
+            U = torch.empty(Ls.gauge, dtype=torch.complex128, device="cuda")
+            q.gauge_random(U, small, 1, EPS, GAUGE_SEED)
+            b = torch.empty(Ls.full, dtype=torch.complex128, device="cuda")
+            q.fermion_random(b, b.numel(), 0, SRC_SEED)
+            x = torch.zeros_like(b)
+            par, grid = q.QcuParam(small), q.QcuParam([1, 1, 1, 1])
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ref.ncclBistabCgQcu(x.data_ptr(), b.data_ptr(), U.data_ptr(), ctypes.byref(par), ctypes.byref(grid))
+            torch.cuda.synchronize()
+            out["ncclBistabCgQcu_s_16x16x16x32_kappa0.125"] = round(time.perf_counter() - t0, 4)
+            return out
+        finally:
+            sys.stdout.flush()
+            os.dup2(saved, 1)
+            os.close(saved)
+            os.close(devnull)
+    except Exception as e:  # the timing is informative; the arm's value is the CPU one
+        return {"error": str(e)[:200]}
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -204,13 +300,18 @@ def run_reference(args, world, rank, pg):
     U = O.gauge_smooth(latt, EPS, GAUGE_SEED)
     b = O.fermion_gauss(O.full_shape(latt), SRC_SEED)
     cb = cpu_sample(latt, args.kappa, U, b, PLAIN_ITERS_REF, budget_s=max(5.0, 60.0 / max(args.steps + args.warmup, 1)))
+    extra = {"cpu_dslash": cpu_dslash_medians(latt)}
+    rg = reference_gpu(latt) if latt == LATT else None
+    if rg is not None:
+        extra["reference_gpu"] = rg
     line = {"metric": METRIC, "value": cb["value"], "unit": "s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["value"] * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic (seeded)",
             "config": {"workload": "wilson-bicgstab-32^3x64-smooth-eps0.25", "latt": latt, "kappa": args.kappa,
                        "tol": TOL, "t_boundary": T_BC},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": cb["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": cb["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            **extra}
     print(json.dumps(line), flush=True)
 
 
@@ -431,6 +532,7 @@ def run_ours(args, world, rank, local, pg):
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_sample(latt, args.kappa, gauge.cpu().numpy(), b.cpu().numpy(), plain_info["iterations"])
         cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu["dslash"] = cpu_dslash_medians(latt)
 
     if rank == 0:
         chosen = infos[-1]
