@@ -38,8 +38,9 @@ EPS = 0.25
 T_BC = -1.0
 GAUGE_SEED = 20251203
 SRC_SEED = 7
-KAPPA = 0.1303            # plain FP64 BiCGSTAB: 620 iterations on this ensemble (0.1304: no convergence in 4000)
-PLAIN_ITERS_REF = 620     # plain FP64 iterations of this system (measured), used to extrapolate CPU samples
+KAPPA = 0.1303            # plain FP64 BiCGSTAB: 620-870 iterations on this ensemble, by summation order (0.1304: no convergence in 4000)
+PLAIN_ITERS_REF = 865     # the CPU oracle's own FP64 BiCGSTAB: 865 iterations to 1e-10 on this system (run once
+                          # to the end: 358 s on 8 cores); the reference arm extrapolates its sample to it
 TOL = 1e-10
 CSW = 1.0
 KAPPA_CLOVER = 0.1291     # clover csw = 1 on the same field: near-critical (plain FP64 ~1000 iterations)
