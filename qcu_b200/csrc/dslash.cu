@@ -12,6 +12,7 @@
 //     and one of  <rt, out>,  <out, x1> & |out|^2,  |out|^2  reduced to the solver state.
 #include <algorithm>
 
+#include "hop32.cuh"
 #include "internal.h"
 
 namespace qcu {
@@ -21,13 +22,78 @@ namespace qcu {
 // 3 blocks fit in 170 registers without spills.  The variants with a reduction
 // stride over the sites with one resident wave of 3 blocks per SM (forcing the
 // 16/32-bit ones to 128 registers for a 4th block measured slower).
-#define DSLASH_MIN_BLOCKS(K, RED) (((K) == AOS64 || (K) == SOA64) ? 3 : 1)
-// resident blocks per SM of the reducing variants (grid of the strided launch)
-#define DSLASH_RED_BLOCKS_PER_SM 3
+// The FP32-spinor kernels (paired FP32 instructions, hop32.cuh) issue few
+// enough instructions to be bound by memory latency instead: they take more
+// resident blocks (72 registers, 7 blocks of 128 threads) for more loads in flight.
+#ifndef QCU_DSLASH32_BLOCKS
+#define QCU_DSLASH32_BLOCKS 7  // FP32 spinors without a reduction
+#endif
+#ifndef QCU_DSLASH32_RED_BLOCKS
+#define QCU_DSLASH32_RED_BLOCKS 3  // FP32 spinors with a reduction
+#endif
+#define DSLASH_RED_BLOCKS(K) ((K) == SOA32 ? QCU_DSLASH32_RED_BLOCKS : 3)
+#define DSLASH_MIN_BLOCKS(K, RED) \
+  (((K) == AOS64 || (K) == SOA64) ? 3 : ((K) == SOA32 ? ((RED) == RED_NONE ? QCU_DSLASH32_BLOCKS : DSLASH_RED_BLOCKS(K)) : 1))
+
+// FP32 spinors: the hop and the epilogue on spin-paired registers (hop32.cuh)
+template <int G, int C, bool CLOV, int NX, int RED, int NV>
+__device__ __forceinline__ void dslash_site32(const Geom &g, const DslashArgs &a, int s, double (&red)[NV]) {
+  const SpinorView<SOA32> in{const_cast<void *>(a.in), nullptr, g.Vh};
+  const GaugeView<G> U{a.gauge, pad_sites(g.Vh)};
+  Site2 w;
+  const float unit = wilson_hop_site2<G>(w, in, U, g, s, a.parity, (float)a.t_bc);
+  if constexpr (CLOV) {
+    Cpx<float> v[12];
+    site2_to_cpx(w, v);
+    clover_apply_site<C, float>(CloverView<C>{a.clover, g.Vh}, s, v);
+    cpx_to_site2(v, w);
+  }
+  site2_scale(w, bc2((float)a.a * unit));
+  Site2 x1;
+  if constexpr (NX >= 1) {
+    site2_load(SpinorView<SOA32>{const_cast<void *>(a.x1), nullptr, g.Vh}, s, x1);
+    site2_axpy(w, bc2((float)a.b1), x1);
+  }
+  if constexpr (NX >= 2) {
+    Site2 x2;
+    site2_load(SpinorView<SOA32>{const_cast<void *>(a.x2), nullptr, g.Vh}, s, x2);
+    site2_axpy(w, bc2((float)a.b2), x2);
+  }
+  site2_store(SpinorView<SOA32>{a.out, nullptr, g.Vh}, s, w);
+  if constexpr (RED != RED_NONE) {
+    Cpx<float> wv[12];
+    site2_to_cpx(w, wv);
+    if constexpr (RED == RED_DOT_RT) {  // <rt, out>
+      Cpx<float> rt[12];
+      spinor_load<SOA32, float>(SpinorView<SOA32>{const_cast<void *>(a.rt), nullptr, g.Vh}, s, rt);
+      site_dot<float>(rt, wv, red[0], red[1]);
+    } else if constexpr (RED == RED_TS_TT) {  // <out, x1>, |out|^2
+      Cpx<float> xv[12];
+      site2_to_cpx(x1, xv);
+      site_dot<float>(wv, xv, red[0], red[1]);
+      site_norm2<float>(wv, red[2]);
+    } else if constexpr (RED == RED_NORM) {
+      site_norm2<float>(wv, red[0]);
+    }
+  }
+}
+
+template <int K, int G, int C, bool CLOV, int NX, int RED, int NV>
+__device__ __forceinline__ void dslash_site_scalar(const Geom &g, const DslashArgs &a, int s, double (&red)[NV]);
 
 // one output site: hop term, clover, epilogue, the site's share of the reduction
 template <int K, int G, int C, bool CLOV, int NX, int RED, int NV>
 __device__ __forceinline__ void dslash_site(const Geom &g, const DslashArgs &a, int s, double (&red)[NV]) {
+  if constexpr (K == SOA32) {
+    dslash_site32<G, C, CLOV, NX, RED, NV>(g, a, s, red);
+  } else {
+    dslash_site_scalar<K, G, C, CLOV, NX, RED, NV>(g, a, s, red);
+  }
+}
+
+// FP64 and 16-bit spinors: scalar complex arithmetic
+template <int K, int G, int C, bool CLOV, int NX, int RED, int NV>
+__device__ __forceinline__ void dslash_site_scalar(const Geom &g, const DslashArgs &a, int s, double (&red)[NV]) {
   using T = typename SpinorReal<K>::T;
   Cpx<T> w[12];
   const SpinorView<K> in{const_cast<void *>(a.in), const_cast<float *>(a.in_norm), g.Vh};
@@ -88,7 +154,7 @@ template <int K, int G, int C, bool CLOV, int NX, int RED>
 static void launch_t(const Geom &g, const DslashArgs &a, Context &ctx, cudaStream_t s) {
   int blocks = (g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK;
   // reductions: one resident wave (the 16/32-bit reducing variants take ~167 registers, FP64 170)
-  if (RED != RED_NONE) blocks = std::min(blocks, DSLASH_RED_BLOCKS_PER_SM * ctx.sms);
+  if (RED != RED_NONE) blocks = std::min(blocks, DSLASH_RED_BLOCKS(K) * ctx.sms);
   RedCtx rc{ctx.st, ctx.partials, a.fin};
   if (RED != RED_NONE) {
     require(a.gate == GATE_ALWAYS || ctx.st != nullptr, "reduction without solver state");

@@ -13,9 +13,11 @@
 //           (python/PyQuda/pyquda/field.py:78,230) -- used by the legacy ABI
 //           so a single dslash needs no layout conversion at all.
 //   SOA64 : double2, NC = 12 (one complex per 16-byte load)
-//   SOA32 : float4,  NC = 6  (two complex per 16-byte load)
+//   SOA32 : float4,  NC = 6: float4 j = 3 * q + c holds colour c of spins 2q
+//           and 2q + 1 as (re, re, im, im), the lane pairs of the paired FP32
+//           instructions (hop32.cuh)
 //   SOA16 : uint4,   NC = 3  + float norm[Vh]: 16-bit fixed point
-//           (int16, value/norm * 32767) scaled by the per-site max |component|,
+//           (offset-binary 16-bit, value/norm * 32767) scaled by the per-site max |component|,
 //           four complex per 16-byte load.  Fixed point keeps 15 bits of
 //           mantissa relative to the site maximum where FP16 keeps 11.
 // Gauge kinds (reconstruct-12: rows 0 and 1 stored, row 2 = conj(r0 x r1),
@@ -23,7 +25,7 @@
 //   GAOS64 : PyQuda layout complex128 [dir][par][site][3][3], rows 0-1 read
 //   GSOA64 : double2, NC = 6
 //   GSOA32 : float4,  NC = 3
-//   GSOA16 : uint2,   NC = 3   (four int16 fixed point per load, |U_ij| <= 1)
+//   GSOA16 : uint2,   NC = 3   (four 16-bit fixed point per load, |U_ij| <= 1)
 #pragma once
 #include "cplx.cuh"
 
@@ -36,20 +38,19 @@ template <int K> struct SpinorReal { using T = float; };
 template <> struct SpinorReal<AOS64> { using T = double; };
 template <> struct SpinorReal<SOA64> { using T = double; };
 
-// 16-bit fixed point: two signed 16-bit values per 32-bit word
+// 16-bit fixed point: two values per 32-bit word, each stored offset-binary
+// (u = v + 32768, v = round(x * 32767) in [-32767, 32767]).
 constexpr float FIX16_SCALE = 32767.0f;
 __device__ __forceinline__ unsigned fix16_pack(float a, float b) {
   const int ia = __float2int_rn(a * FIX16_SCALE), ib = __float2int_rn(b * FIX16_SCALE);
-  return ((unsigned)ia & 0xffffu) | ((unsigned)ib << 16);
+  return (((unsigned)ia & 0xffffu) | ((unsigned)ib << 16)) ^ 0x80008000u;
 }
-// decode without int->float conversions: flipping the sign bits turns each
-// signed half into an offset-binary u = v + 32768; byte-permuting u under the
-// exponent bits of 2^23 gives the float 2^23 + u exactly, and subtracting
-// 2^23 + 32768 (exact, same exponent) leaves v.
+// decode without int->float conversions: byte-permuting u under the exponent
+// bits of 2^23 gives the float 2^23 + u exactly, and subtracting 2^23 + 32768
+// (exact, same exponent) leaves v -- one PRMT and one FADD per value.
 __device__ __forceinline__ float2 fix16_unpack(unsigned w) {
-  const unsigned x = w ^ 0x80008000u;
-  const float lo = __int_as_float(__byte_perm(x, 0x4B000000u, 0x7610)) - 8421376.0f;
-  const float hi = __int_as_float(__byte_perm(x, 0x4B000000u, 0x7632)) - 8421376.0f;
+  const float lo = __int_as_float(__byte_perm(w, 0x4B000000u, 0x7610)) - 8421376.0f;
+  const float hi = __int_as_float(__byte_perm(w, 0x4B000000u, 0x7632)) - 8421376.0f;
   return make_float2(lo, hi);
 }
 
@@ -96,10 +97,11 @@ __device__ __forceinline__ void spinor_load(const SpinorView<K> &v, int s, Cpx<T
   } else if constexpr (K == SOA32) {
     const float4 *p = static_cast<const float4 *>(v.p) + blk_base<6>(s);
 #pragma unroll
-    for (int c = 0; c < 6; c++) {
-      float4 d = __ldg(p + c * SB);
-      out[2 * c] = Cpx<T>((T)d.x, (T)d.y);
-      out[2 * c + 1] = Cpx<T>((T)d.z, (T)d.w);
+    for (int j = 0; j < 6; j++) {  // j = 3 * (spin pair) + colour
+      float4 d = __ldg(p + j * SB);
+      const int a = (j / 3) * 6 + j % 3;  // spin 2 * (j / 3), then spin 2 * (j / 3) + 1
+      out[a] = Cpx<T>((T)d.x, (T)d.z);
+      out[a + 3] = Cpx<T>((T)d.y, (T)d.w);
     }
   } else {
     const uint4 *p = static_cast<const uint4 *>(v.p) + blk_base<3>(s);
@@ -146,8 +148,10 @@ __device__ __forceinline__ void spinor_store(const SpinorView<K> &v, int s, cons
   } else if constexpr (K == SOA32) {
     float4 *p = static_cast<float4 *>(v.p) + blk_base<6>(s);
 #pragma unroll
-    for (int c = 0; c < 6; c++)
-      p[c * SB] = make_float4((float)in[2 * c].re, (float)in[2 * c].im, (float)in[2 * c + 1].re, (float)in[2 * c + 1].im);
+    for (int j = 0; j < 6; j++) {
+      const int a = (j / 3) * 6 + j % 3;
+      p[j * SB] = make_float4((float)in[a].re, (float)in[a + 3].re, (float)in[a].im, (float)in[a + 3].im);
+    }
   } else {
     float mx = 0.f;
 #pragma unroll

@@ -1,0 +1,321 @@
+// FP32 hopping term on spin-paired registers.
+//
+// sm_100 issues two FP32 lanes per instruction (FFMA2 / FADD2 / FMUL2 on a
+// float2).  The FP32 spinor storage (SOA32) keeps spins 0 and 1 -- and spins 2
+// and 3 -- of one colour side by side, so a 16-byte load yields two such lane
+// pairs, (re s0, re s1) and (im s0, im s1).  The rank-2 projector of the z and
+// t hops combines spin 0 with 2 and spin 1 with 3, lane by lane; the x and y
+// hops cross the lanes (0 with 3, 1 with 2) and are projected and
+// reconstructed with scalar instructions.  The colour matrix-vector product,
+// the largest share of the arithmetic, acts on both spins of the projected
+// half spinor at once: every link element is held as a broadcast pair
+// (u, u), built once per hop, and multiplies the pair (h0, h1).  The same
+// arithmetic as the scalar hop (src/wilson_dslash.cu:56-243 of qcu), with half
+// the FP32 instructions in the projection, the product and the reconstruction.
+#pragma once
+#include "fields.cuh"
+
+namespace qcu {
+
+// One colour triplet of two spins, as lane pairs: re[c] = (re of spin a, re of
+// spin b), im[c] likewise.
+struct SpinPair {
+  float2 re[3], im[3];
+};
+// One FP32 site: spins (0,1) and (2,3).
+struct Site2 {
+  SpinPair up, lo;
+};
+// One SU(3) link with every element broadcast to both lanes: re[r*3+c] = (Re U_rc, Re U_rc).
+struct Link2 {
+  float2 re[9], im[9];
+};
+
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+// a * (k0, k1) + c with compile-time constants k in {-1, 1}
+template <int K0, int K1>
+__device__ __forceinline__ float2 fmak(float2 a, float2 c) {
+  if constexpr (K0 == 1 && K1 == 1) return add2(c, a);
+  else if constexpr (K0 == -1 && K1 == -1) return add2(c, neg2(a));
+  else return fma2(a, make_float2((float)K0, (float)K1), c);
+}
+
+// ------------------------------------------------------------------ SOA32 site I/O
+__device__ __forceinline__ void site2_load(const SpinorView<SOA32> &v, int s, Site2 &o) {
+  const float4 *p = static_cast<const float4 *>(v.p) + blk_base<6>(s);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const float4 d = __ldg(p + c * SB), e = __ldg(p + (3 + c) * SB);
+    o.up.re[c] = make_float2(d.x, d.y);
+    o.up.im[c] = make_float2(d.z, d.w);
+    o.lo.re[c] = make_float2(e.x, e.y);
+    o.lo.im[c] = make_float2(e.z, e.w);
+  }
+}
+
+__device__ __forceinline__ void site2_store(const SpinorView<SOA32> &v, int s, const Site2 &w) {
+  float4 *p = static_cast<float4 *>(v.p) + blk_base<6>(s);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    p[c * SB] = make_float4(w.up.re[c].x, w.up.re[c].y, w.up.im[c].x, w.up.im[c].y);
+    p[(3 + c) * SB] = make_float4(w.lo.re[c].x, w.lo.re[c].y, w.lo.im[c].x, w.lo.im[c].y);
+  }
+}
+
+// canonical component order (spin * 3 + colour) <-> lane pairs; register renaming only
+__device__ __forceinline__ void site2_to_cpx(const Site2 &w, Cpx<float> v[12]) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    v[c] = Cpx<float>(w.up.re[c].x, w.up.im[c].x);
+    v[3 + c] = Cpx<float>(w.up.re[c].y, w.up.im[c].y);
+    v[6 + c] = Cpx<float>(w.lo.re[c].x, w.lo.im[c].x);
+    v[9 + c] = Cpx<float>(w.lo.re[c].y, w.lo.im[c].y);
+  }
+}
+__device__ __forceinline__ void cpx_to_site2(const Cpx<float> v[12], Site2 &w) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    w.up.re[c] = make_float2(v[c].re, v[3 + c].re);
+    w.up.im[c] = make_float2(v[c].im, v[3 + c].im);
+    w.lo.re[c] = make_float2(v[6 + c].re, v[9 + c].re);
+    w.lo.im[c] = make_float2(v[6 + c].im, v[9 + c].im);
+  }
+}
+
+__device__ __forceinline__ void site2_scale(Site2 &w, float2 f) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    w.up.re[c] = mul2(w.up.re[c], f);
+    w.up.im[c] = mul2(w.up.im[c], f);
+    w.lo.re[c] = mul2(w.lo.re[c], f);
+    w.lo.im[c] = mul2(w.lo.im[c], f);
+  }
+}
+// w += f * x
+__device__ __forceinline__ void site2_axpy(Site2 &w, float2 f, const Site2 &x) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    w.up.re[c] = fma2(x.up.re[c], f, w.up.re[c]);
+    w.up.im[c] = fma2(x.up.im[c], f, w.up.im[c]);
+    w.lo.re[c] = fma2(x.lo.re[c], f, w.lo.re[c]);
+    w.lo.im[c] = fma2(x.lo.im[c], f, w.lo.im[c]);
+  }
+}
+
+// ------------------------------------------------------------------ links
+// row 2 = conj(row0 x row1), on broadcast pairs (k = 3 * r + c)
+__device__ __forceinline__ void link2_row2(Link2 &m) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int a = (c + 1) % 3, b = (c + 2) % 3;  // m[2][c] = conj(m0a m1b - m0b m1a)
+    float2 re = mul2(m.re[a], m.re[3 + b]);
+    re = fma2(neg2(m.im[a]), m.im[3 + b], re);
+    re = fma2(neg2(m.re[b]), m.re[3 + a], re);
+    re = fma2(m.im[b], m.im[3 + a], re);
+    float2 im = mul2(neg2(m.re[a]), m.im[3 + b]);
+    im = fma2(neg2(m.im[a]), m.re[3 + b], im);
+    im = fma2(m.re[b], m.im[3 + a], im);
+    im = fma2(m.im[b], m.re[3 + a], im);
+    m.re[6 + c] = re;
+    m.im[6 + c] = im;
+  }
+}
+
+// GSOA32: rows 0-1 as stored, row 2 rebuilt.  Returns the unit of the
+// elements (1).
+// GSOA16: rows 0-1 in units of 1/32767, row 2 rebuilt and brought to the same
+// unit.  Returns the unit (1/32767), applied once to the whole hop sum.
+template <int G>
+__device__ __forceinline__ float link2_load(const GaugeView<G> &u, int dir, int par, int s, Link2 &m) {
+  const size_t slab = (size_t)(dir * 2 + par) * u.stride;
+  if constexpr (G == GSOA32) {
+    const float4 *p = static_cast<const float4 *>(u.p) + slab * 3 + blk_base<3>(s);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const float4 d = __ldg(p + k * SB);
+      m.re[2 * k] = bc2(d.x);
+      m.im[2 * k] = bc2(d.y);
+      m.re[2 * k + 1] = bc2(d.z);
+      m.im[2 * k + 1] = bc2(d.w);
+    }
+    link2_row2(m);
+    return 1.0f;
+  } else {
+    static_assert(G == GSOA16, "FP32 hop: GSOA32 or GSOA16 links");
+    const uint2 *p = static_cast<const uint2 *>(u.p) + slab * 3 + blk_base<3>(s);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const uint2 d = __ldg(p + k * SB);
+      const float2 a = fix16_unpack(d.x), b = fix16_unpack(d.y);
+      m.re[2 * k] = bc2(a.x);
+      m.im[2 * k] = bc2(a.y);
+      m.re[2 * k + 1] = bc2(b.x);
+      m.im[2 * k + 1] = bc2(b.y);
+    }
+    link2_row2(m);
+    const float2 unit = bc2(1.0f / FIX16_SCALE);
+#pragma unroll
+    for (int k = 6; k < 9; k++) {
+      m.re[k] = mul2(m.re[k], unit);
+      m.im[k] = mul2(m.im[k], unit);
+    }
+    return 1.0f / FIX16_SCALE;
+  }
+}
+
+// ------------------------------------------------------------------ one hop
+// acc += U (1 - gamma_mu) psi (FWD) or U^dag (1 + gamma_mu) psi (!FWD), times
+// ph (the time-boundary phase; 1 for mu < 3).  Gamma conventions as gcol /
+// gre / gim in fields.cuh.
+template <int MU, bool FWD>
+__device__ __forceinline__ void hop2(Site2 &acc, const Site2 &psi, const Link2 &u, float ph) {
+  constexpr int S = FWD ? -1 : 1;
+  SpinPair h, uh;
+  // rows 0, 1 of the projector: h_r = psi_r + S g(mu,r) psi_gcol(mu,r)
+  if constexpr (MU >= 2) {  // gcol = 2, 3: lane-aligned with the lower spins
+    constexpr int A0 = S * gre(MU, 0), A1 = S * gre(MU, 1), B0 = S * gim(MU, 0), B1 = S * gim(MU, 1);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      if constexpr (A0 != 0) {
+        h.re[c] = fmak<A0, A1>(psi.lo.re[c], psi.up.re[c]);
+        h.im[c] = fmak<A0, A1>(psi.lo.im[c], psi.up.im[c]);
+      } else {
+        h.re[c] = fmak<-B0, -B1>(psi.lo.im[c], psi.up.re[c]);
+        h.im[c] = fmak<B0, B1>(psi.lo.re[c], psi.up.im[c]);
+      }
+    }
+  } else {  // gcol = 3, 2: crossed lanes, scalar
+#pragma unroll
+    for (int c = 0; c < 3; c++) {  // h_0 from spin 3 (lane y), h_1 from spin 2 (lane x)
+      const Cpx<float> q0 = unit_mul<S * gre(MU, 0), S * gim(MU, 0)>(Cpx<float>(psi.lo.re[c].y, psi.lo.im[c].y));
+      const Cpx<float> q1 = unit_mul<S * gre(MU, 1), S * gim(MU, 1)>(Cpx<float>(psi.lo.re[c].x, psi.lo.im[c].x));
+      h.re[c] = make_float2(psi.up.re[c].x + q0.re, psi.up.re[c].y + q1.re);
+      h.im[c] = make_float2(psi.up.im[c].x + q0.im, psi.up.im[c].y + q1.im);
+    }
+  }
+  if constexpr (MU == 3) {
+    const float2 f = bc2(ph);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      h.re[c] = mul2(h.re[c], f);
+      h.im[c] = mul2(h.im[c], f);
+    }
+  }
+  // colour product on both spins at once
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    float2 re, im;
+    if constexpr (FWD) {  // U h
+      re = mul2(u.re[r * 3], h.re[0]);
+      im = mul2(u.re[r * 3], h.im[0]);
+      re = fma2(neg2(u.im[r * 3]), h.im[0], re);
+      im = fma2(u.im[r * 3], h.re[0], im);
+#pragma unroll
+      for (int c = 1; c < 3; c++) {
+        re = fma2(u.re[r * 3 + c], h.re[c], re);
+        im = fma2(u.re[r * 3 + c], h.im[c], im);
+        re = fma2(neg2(u.im[r * 3 + c]), h.im[c], re);
+        im = fma2(u.im[r * 3 + c], h.re[c], im);
+      }
+    } else {  // U^dag h
+      re = mul2(u.re[r], h.re[0]);
+      im = mul2(u.re[r], h.im[0]);
+      re = fma2(u.im[r], h.im[0], re);
+      im = fma2(neg2(u.im[r]), h.re[0], im);
+#pragma unroll
+      for (int c = 1; c < 3; c++) {
+        re = fma2(u.re[c * 3 + r], h.re[c], re);
+        im = fma2(u.re[c * 3 + r], h.im[c], im);
+        re = fma2(u.im[c * 3 + r], h.im[c], re);
+        im = fma2(neg2(u.im[c * 3 + r]), h.re[c], im);
+      }
+    }
+    uh.re[r] = re;
+    uh.im[r] = im;
+  }
+  // rows 0, 1 of the result; rows 2, 3 = S g(mu,r) uh_gcol(mu,r)
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    acc.up.re[c] = add2(acc.up.re[c], uh.re[c]);
+    acc.up.im[c] = add2(acc.up.im[c], uh.im[c]);
+  }
+  if constexpr (MU >= 2) {  // gcol = 0, 1: lane-aligned
+    constexpr int A2 = S * gre(MU, 2), A3 = S * gre(MU, 3), B2 = S * gim(MU, 2), B3 = S * gim(MU, 3);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      if constexpr (A2 != 0) {
+        acc.lo.re[c] = fmak<A2, A3>(uh.re[c], acc.lo.re[c]);
+        acc.lo.im[c] = fmak<A2, A3>(uh.im[c], acc.lo.im[c]);
+      } else {
+        acc.lo.re[c] = fmak<-B2, -B3>(uh.im[c], acc.lo.re[c]);
+        acc.lo.im[c] = fmak<B2, B3>(uh.re[c], acc.lo.im[c]);
+      }
+    }
+  } else {  // gcol = 1, 0: crossed lanes, scalar
+#pragma unroll
+    for (int c = 0; c < 3; c++) {  // row 2 from uh_1 (lane y), row 3 from uh_0 (lane x)
+      const Cpx<float> v2 = unit_mul<S * gre(MU, 2), S * gim(MU, 2)>(Cpx<float>(uh.re[c].y, uh.im[c].y));
+      const Cpx<float> v3 = unit_mul<S * gre(MU, 3), S * gim(MU, 3)>(Cpx<float>(uh.re[c].x, uh.im[c].x));
+      acc.lo.re[c].x += v2.re;
+      acc.lo.im[c].x += v2.im;
+      acc.lo.re[c].y += v3.re;
+      acc.lo.im[c].y += v3.im;
+    }
+  }
+}
+
+template <int MU, bool FWD, int G>
+__device__ __forceinline__ float hop2_from(Site2 &acc, const SpinorView<SOA32> &in, const GaugeView<G> &U, int n,
+                                           int lpar, int ls, float ph) {
+  Site2 psi;
+  Link2 u;
+  site2_load(in, n, psi);
+  const float unit = link2_load<G>(U, MU, lpar, ls, u);
+  hop2<MU, FWD>(acc, psi, u, ph);
+  return unit;
+}
+
+// Hopping term D_{p <- 1-p} at output site s of parity par, FP32 spinors:
+// acc = the sum over the eight hops in units of the returned value (1/32767
+// for 16-bit links, 1 for FP32 links), which the caller folds into its own
+// scale factor.  Neighbour indexing as wilson_hop_site.
+template <int G>
+__device__ __forceinline__ float wilson_hop_site2(Site2 &acc, const SpinorView<SOA32> &in, const GaugeView<G> &U,
+                                                  const Geom &g, int s, int par, float t_bc) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    acc.up.re[c] = acc.up.im[c] = acc.lo.re[c] = acc.lo.im[c] = make_float2(0.f, 0.f);
+  }
+  const int xh = s % g.Lxh;
+  int r = s / g.Lxh;
+  const int y = r % g.Ly;
+  r /= g.Ly;
+  const int z = r % g.Lz;
+  const int t = r / g.Lz;
+  const int xodd = (y + z + t + par) & 1;
+  int n;
+  float unit;
+  n = xodd ? (xh == g.Lxh - 1 ? s - xh : s + 1) : s;
+  unit = hop2_from<0, true>(acc, in, U, n, par, s, 1.f);
+  n = xodd ? s : (xh == 0 ? s + g.Lxh - 1 : s - 1);
+  hop2_from<0, false>(acc, in, U, n, 1 - par, n, 1.f);
+  n = (y == g.Ly - 1) ? s - (g.Ly - 1) * g.sy : s + g.sy;
+  hop2_from<1, true>(acc, in, U, n, par, s, 1.f);
+  n = (y == 0) ? s + (g.Ly - 1) * g.sy : s - g.sy;
+  hop2_from<1, false>(acc, in, U, n, 1 - par, n, 1.f);
+  n = (z == g.Lz - 1) ? s - (g.Lz - 1) * g.sz : s + g.sz;
+  hop2_from<2, true>(acc, in, U, n, par, s, 1.f);
+  n = (z == 0) ? s + (g.Lz - 1) * g.sz : s - g.sz;
+  hop2_from<2, false>(acc, in, U, n, 1 - par, n, 1.f);
+  n = (t == g.Lt - 1) ? s - (g.Lt - 1) * g.st : s + g.st;
+  hop2_from<3, true>(acc, in, U, n, par, s, (t == g.Lt - 1) ? t_bc : 1.f);
+  n = (t == 0) ? s + (g.Lt - 1) * g.st : s - g.st;
+  hop2_from<3, false>(acc, in, U, n, 1 - par, n, (t == 0) ? t_bc : 1.f);
+  return unit;
+}
+
+}  // namespace qcu
