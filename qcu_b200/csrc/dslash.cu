@@ -22,26 +22,28 @@ namespace qcu {
 // 3 blocks fit in 170 registers without spills.  The variants with a reduction
 // stride over the sites with one resident wave of 3 blocks per SM (forcing the
 // 16/32-bit ones to 128 registers for a 4th block measured slower).
-// The FP32-spinor kernels (paired FP32 instructions, hop32.cuh) issue few
-// enough instructions to be bound by memory latency instead: they take more
-// resident blocks (72 registers, 7 blocks of 128 threads) for more loads in flight.
+// The FP32- and 16-bit-spinor kernels (paired FP32 instructions, hop32.cuh)
+// issue few enough instructions to be bound by memory latency instead: they
+// take more resident blocks (72 registers, 7 blocks of 128 threads) for more
+// loads in flight.
 #ifndef QCU_DSLASH32_BLOCKS
-#define QCU_DSLASH32_BLOCKS 7  // FP32 spinors without a reduction
+#define QCU_DSLASH32_BLOCKS 7  // FP32 / 16-bit spinors without a reduction
 #endif
 #ifndef QCU_DSLASH32_RED_BLOCKS
-#define QCU_DSLASH32_RED_BLOCKS 3  // FP32 spinors with a reduction
+#define QCU_DSLASH32_RED_BLOCKS 3  // FP32 / 16-bit spinors with a reduction
 #endif
-#define DSLASH_RED_BLOCKS(K) ((K) == SOA32 ? QCU_DSLASH32_RED_BLOCKS : 3)
+#define DSLASH_RED_BLOCKS(K) (((K) == SOA32 || (K) == SOA16) ? QCU_DSLASH32_RED_BLOCKS : 3)
 #define DSLASH_MIN_BLOCKS(K, RED) \
-  (((K) == AOS64 || (K) == SOA64) ? 3 : ((K) == SOA32 ? ((RED) == RED_NONE ? QCU_DSLASH32_BLOCKS : DSLASH_RED_BLOCKS(K)) : 1))
+  (((K) == AOS64 || (K) == SOA64) ? 3 : ((RED) == RED_NONE ? QCU_DSLASH32_BLOCKS : DSLASH_RED_BLOCKS(K)))
 
-// FP32 spinors: the hop and the epilogue on spin-paired registers (hop32.cuh)
-template <int G, int C, bool CLOV, int NX, int RED, int NV>
+// FP32 and 16-bit spinors: the hop and the epilogue on spin-paired registers
+// in FP32 arithmetic (hop32.cuh)
+template <int K, int G, int C, bool CLOV, int NX, int RED, int NV>
 __device__ __forceinline__ void dslash_site32(const Geom &g, const DslashArgs &a, int s, double (&red)[NV]) {
-  const SpinorView<SOA32> in{const_cast<void *>(a.in), nullptr, g.Vh};
+  const SpinorView<K> in{const_cast<void *>(a.in), const_cast<float *>(a.in_norm), g.Vh};
   const GaugeView<G> U{a.gauge, pad_sites(g.Vh)};
   Site2 w;
-  const float unit = wilson_hop_site2<G>(w, in, U, g, s, a.parity, (float)a.t_bc);
+  const float unit = wilson_hop_site2<K, G>(w, in, U, g, s, a.parity, (float)a.t_bc);
   if constexpr (CLOV) {
     Cpx<float> v[12];
     site2_to_cpx(w, v);
@@ -51,21 +53,21 @@ __device__ __forceinline__ void dslash_site32(const Geom &g, const DslashArgs &a
   site2_scale(w, bc2((float)a.a * unit));
   Site2 x1;
   if constexpr (NX >= 1) {
-    site2_load(SpinorView<SOA32>{const_cast<void *>(a.x1), nullptr, g.Vh}, s, x1);
+    site_load2<K>(SpinorView<K>{const_cast<void *>(a.x1), const_cast<float *>(a.x1_norm), g.Vh}, s, x1);
     site2_axpy(w, bc2((float)a.b1), x1);
   }
   if constexpr (NX >= 2) {
     Site2 x2;
-    site2_load(SpinorView<SOA32>{const_cast<void *>(a.x2), nullptr, g.Vh}, s, x2);
+    site_load2<K>(SpinorView<K>{const_cast<void *>(a.x2), const_cast<float *>(a.x2_norm), g.Vh}, s, x2);
     site2_axpy(w, bc2((float)a.b2), x2);
   }
-  site2_store(SpinorView<SOA32>{a.out, nullptr, g.Vh}, s, w);
+  site_store2<K>(SpinorView<K>{a.out, a.out_norm, g.Vh}, s, w);
   if constexpr (RED != RED_NONE) {
     Cpx<float> wv[12];
     site2_to_cpx(w, wv);
     if constexpr (RED == RED_DOT_RT) {  // <rt, out>
       Cpx<float> rt[12];
-      spinor_load<SOA32, float>(SpinorView<SOA32>{const_cast<void *>(a.rt), nullptr, g.Vh}, s, rt);
+      spinor_load<K, float>(SpinorView<K>{const_cast<void *>(a.rt), const_cast<float *>(a.rt_norm), g.Vh}, s, rt);
       site_dot<float>(rt, wv, red[0], red[1]);
     } else if constexpr (RED == RED_TS_TT) {  // <out, x1>, |out|^2
       Cpx<float> xv[12];
@@ -84,14 +86,14 @@ __device__ __forceinline__ void dslash_site_scalar(const Geom &g, const DslashAr
 // one output site: hop term, clover, epilogue, the site's share of the reduction
 template <int K, int G, int C, bool CLOV, int NX, int RED, int NV>
 __device__ __forceinline__ void dslash_site(const Geom &g, const DslashArgs &a, int s, double (&red)[NV]) {
-  if constexpr (K == SOA32) {
-    dslash_site32<G, C, CLOV, NX, RED, NV>(g, a, s, red);
+  if constexpr (K == SOA32 || K == SOA16) {
+    dslash_site32<K, G, C, CLOV, NX, RED, NV>(g, a, s, red);
   } else {
     dslash_site_scalar<K, G, C, CLOV, NX, RED, NV>(g, a, s, red);
   }
 }
 
-// FP64 and 16-bit spinors: scalar complex arithmetic
+// FP64 spinors: scalar complex arithmetic
 template <int K, int G, int C, bool CLOV, int NX, int RED, int NV>
 __device__ __forceinline__ void dslash_site_scalar(const Geom &g, const DslashArgs &a, int s, double (&red)[NV]) {
   using T = typename SpinorReal<K>::T;

@@ -17,8 +17,9 @@
 //           and 2q + 1 as (re, re, im, im), the lane pairs of the paired FP32
 //           instructions (hop32.cuh)
 //   SOA16 : uint4,   NC = 3  + float norm[Vh]: 16-bit fixed point
-//           (offset-binary 16-bit, value/norm * 32767) scaled by the per-site max |component|,
-//           four complex per 16-byte load.  Fixed point keeps 15 bits of
+//           (offset-binary 16-bit, value/norm * 32767) scaled by the per-site max |component|;
+//           word k = 6 q + 2 c + (re, im) holds spin 2q (low half) and 2q + 1 (high
+//           half) of colour c, eight values per 16-byte load.  Fixed point keeps 15 bits of
 //           mantissa relative to the site maximum where FP16 keeps 11.
 // Gauge kinds (reconstruct-12: rows 0 and 1 stored, row 2 = conj(r0 x r1),
 // include/define.h:198-206), one slab of Vh_pad sites per (dir, parity):
@@ -52,6 +53,16 @@ __device__ __forceinline__ float2 fix16_unpack(unsigned w) {
   const float lo = __int_as_float(__byte_perm(w, 0x4B000000u, 0x7610)) - 8421376.0f;
   const float hi = __int_as_float(__byte_perm(w, 0x4B000000u, 0x7632)) - 8421376.0f;
   return make_float2(lo, hi);
+}
+
+// Two values times k into one word (as fix16_pack(a * k / 32767, b * k /
+// 32767)): adding 1.5 * 2^23 + 32768 rounds a float in [-32767, 32767] to the
+// nearest integer in the low mantissa bits, already offset-binary, and one
+// byte permute takes the two low halves.
+constexpr float FIX16_ROUND = 12615680.0f;  // 1.5 * 2^23 + 32768
+__device__ __forceinline__ unsigned fix16_pack_k(float a, float b, float k) {
+  const float ra = fmaf(a, k, FIX16_ROUND), rb = fmaf(b, k, FIX16_ROUND);
+  return __byte_perm(__float_as_uint(ra), __float_as_uint(rb), 0x5410);
 }
 
 // site-blocked indexing
@@ -106,33 +117,28 @@ __device__ __forceinline__ void spinor_load(const SpinorView<K> &v, int s, Cpx<T
   } else {
     const uint4 *p = static_cast<const uint4 *>(v.p) + blk_base<3>(s);
     const float nrm = __ldg(v.norm + s) * (1.0f / FIX16_SCALE);
+    unsigned w[12];
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      uint4 d = __ldg(p + c * SB);
-      unsigned w[4] = {d.x, d.y, d.z, d.w};
+    for (int j = 0; j < 3; j++) {
+      const uint4 d = __ldg(p + j * SB);
+      w[4 * j] = d.x;
+      w[4 * j + 1] = d.y;
+      w[4 * j + 2] = d.z;
+      w[4 * j + 3] = d.w;
+    }
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const float2 f = fix16_unpack(w[k]);
-        out[4 * c + k] = Cpx<T>((T)(f.x * nrm), (T)(f.y * nrm));
+    for (int k = 0; k < 12; k++) {  // word k = 6 * (spin pair) + 2 * colour + (re, im)
+      const float2 f = fix16_unpack(w[k]);
+      const int a = (k / 6) * 6 + (k % 6) / 2;
+      if (k % 2 == 0) {
+        out[a].re = (T)(f.x * nrm);
+        out[a + 3].re = (T)(f.y * nrm);
+      } else {
+        out[a].im = (T)(f.x * nrm);
+        out[a + 3].im = (T)(f.y * nrm);
       }
     }
   }
-}
-
-// SOA16 without the per-site scale: values in units of norm/32767, and the norm
-__device__ __forceinline__ float spinor16_load_raw(const SpinorView<SOA16> &v, int s, Cpx<float> out[12]) {
-  const uint4 *p = static_cast<const uint4 *>(v.p) + blk_base<3>(s);
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    uint4 d = __ldg(p + c * SB);
-    unsigned w[4] = {d.x, d.y, d.z, d.w};
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const float2 f = fix16_unpack(w[k]);
-      out[4 * c + k] = Cpx<float>(f.x, f.y);
-    }
-  }
-  return __ldg(v.norm + s);
 }
 
 template <int K, typename T>
@@ -156,15 +162,17 @@ __device__ __forceinline__ void spinor_store(const SpinorView<K> &v, int s, cons
     float mx = 0.f;
 #pragma unroll
     for (int c = 0; c < 12; c++) mx = fmaxf(mx, fmaxf(fabsf((float)in[c].re), fabsf((float)in[c].im)));
-    float inv = mx > 0.f ? 1.0f / mx : 0.f;
+    const float k = mx > 0.f ? FIX16_SCALE / mx : 0.f;
+    unsigned w[12];
+#pragma unroll
+    for (int q = 0; q < 12; q++) {
+      const int a = (q / 6) * 6 + (q % 6) / 2;
+      w[q] = q % 2 == 0 ? fix16_pack_k((float)in[a].re, (float)in[a + 3].re, k)
+                        : fix16_pack_k((float)in[a].im, (float)in[a + 3].im, k);
+    }
     uint4 *p = static_cast<uint4 *>(v.p) + blk_base<3>(s);
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      unsigned w[4];
-#pragma unroll
-      for (int k = 0; k < 4; k++) w[k] = fix16_pack((float)in[4 * c + k].re * inv, (float)in[4 * c + k].im * inv);
-      p[c * SB] = make_uint4(w[0], w[1], w[2], w[3]);
-    }
+    for (int j = 0; j < 3; j++) p[j * SB] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
     v.norm[s] = mx;
   }
 }
@@ -296,30 +304,15 @@ __device__ __forceinline__ void hop(Cpx<T> acc[12], const Cpx<T> psi[12], const 
   }
 }
 
-// One hop: neighbour spinor n, link U_MU on (lpar, ls), boundary phase ph.
-// The 16-bit path multiplies in integer units and applies the spinor norm,
-// both fixed-point scales and the phase once, to the projected product.
+// One hop: neighbour spinor n, link U_MU on (lpar, ls), boundary phase ph
+// (the FP64 kinds; FP32 and 16-bit spinors take the paired path of hop32.cuh).
 template <int MU, bool FWD, int K, int G, typename T>
 __device__ __forceinline__ void hop_from(Cpx<T> acc[12], const SpinorView<K> &in, const GaugeView<G> &U, int n,
                                          int lpar, int ls, T ph) {
-  if constexpr (K == SOA16 && G == GSOA16) {
-    static_assert(sizeof(T) == 4, "16-bit storage computes in FP32");
-    Cpx<float> psi[12], u[9];
-    const float nrm = spinor16_load_raw(in, n, psi);
-    link16_load_raw(U, MU, lpar, ls, u);
-    hop<MU, FWD, true, float>(acc, psi, u, nrm * (1.0f / (FIX16_SCALE * FIX16_SCALE)) * ph);
-  } else if constexpr (K == SOA32 && G == GSOA16) {
-    // FP32 spinors with 16-bit links: the link scale folds into the hop factor
-    Cpx<float> psi[12], u[9];
-    spinor_load<K, float>(in, n, psi);
-    link16_load_raw(U, MU, lpar, ls, u);
-    hop<MU, FWD, true, float>(acc, psi, u, (1.0f / FIX16_SCALE) * ph);
-  } else {
-    Cpx<T> psi[12], u[9];
-    spinor_load<K, T>(in, n, psi);
-    link_load<G, T>(U, MU, lpar, ls, u);
-    hop<MU, FWD, MU == 3, T>(acc, psi, u, ph);
-  }
+  Cpx<T> psi[12], u[9];
+  spinor_load<K, T>(in, n, psi);
+  link_load<G, T>(U, MU, lpar, ls, u);
+  hop<MU, FWD, MU == 3, T>(acc, psi, u, ph);
 }
 
 // Hopping term D_{p <- 1-p} at output site s of parity `par`:

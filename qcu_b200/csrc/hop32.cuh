@@ -1,4 +1,4 @@
-// FP32 hopping term on spin-paired registers.
+// FP32-arithmetic hopping term (FP32 and 16-bit spinors) on spin-paired registers.
 //
 // sm_100 issues two FP32 lanes per instruction (FFMA2 / FADD2 / FMUL2 on a
 // float2).  The FP32 spinor storage (SOA32) keeps spins 0 and 1 -- and spins 2
@@ -12,6 +12,8 @@
 // (u, u), built once per hop, and multiplies the pair (h0, h1).  The same
 // arithmetic as the scalar hop (src/wilson_dslash.cu:56-243 of qcu), with half
 // the FP32 instructions in the projection, the product and the reconstruction.
+// The 16-bit spinors (SOA16) store the same lane pairs in one word each, so
+// one byte permute per value and one paired subtraction per pair decode them.
 #pragma once
 #include "fields.cuh"
 
@@ -106,6 +108,83 @@ __device__ __forceinline__ void site2_axpy(Site2 &w, float2 f, const Site2 &x) {
   }
 }
 
+// ------------------------------------------------------------------ SOA16 site I/O
+// One 16-bit word -> its two values as a lane pair, in units of the stored
+// scale (the decode of fix16_unpack, with one paired subtraction).
+__device__ __forceinline__ float2 fix16_unpack2(unsigned w) {
+  const float2 b = make_float2(__int_as_float(__byte_perm(w, 0x4B000000u, 0x7610)),
+                               __int_as_float(__byte_perm(w, 0x4B000000u, 0x7632)));
+  return add2(b, bc2(-8421376.0f));
+}
+
+// SOA16 site in units of norm/32767 (word k = 6 q + 2 c + (re, im) is the lane
+// pair of spins 2q, 2q + 1); returns the site norm.
+__device__ __forceinline__ float site16_load_raw(const SpinorView<SOA16> &v, int s, Site2 &o) {
+  const uint4 *p = static_cast<const uint4 *>(v.p) + blk_base<3>(s);
+  unsigned w[12];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const uint4 d = __ldg(p + j * SB);
+    w[4 * j] = d.x;
+    w[4 * j + 1] = d.y;
+    w[4 * j + 2] = d.z;
+    w[4 * j + 3] = d.w;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    o.up.re[c] = fix16_unpack2(w[2 * c]);
+    o.up.im[c] = fix16_unpack2(w[2 * c + 1]);
+    o.lo.re[c] = fix16_unpack2(w[6 + 2 * c]);
+    o.lo.im[c] = fix16_unpack2(w[6 + 2 * c + 1]);
+  }
+  return __ldg(v.norm + s);
+}
+
+// pack a lane pair times k (k = 32767 / norm) into one word (fix16_pack_k, paired)
+__device__ __forceinline__ unsigned fix16_pack2(float2 v, float2 k) {
+  const float2 r = fma2(v, k, bc2(FIX16_ROUND));
+  return __byte_perm(__float_as_uint(r.x), __float_as_uint(r.y), 0x5410);
+}
+
+__device__ __forceinline__ void site16_store(const SpinorView<SOA16> &v, int s, const Site2 &x) {
+  float mx = 0.f;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    mx = fmaxf(mx, fmaxf(fmaxf(fabsf(x.up.re[c].x), fabsf(x.up.re[c].y)), fmaxf(fabsf(x.up.im[c].x), fabsf(x.up.im[c].y))));
+    mx = fmaxf(mx, fmaxf(fmaxf(fabsf(x.lo.re[c].x), fabsf(x.lo.re[c].y)), fmaxf(fabsf(x.lo.im[c].x), fabsf(x.lo.im[c].y))));
+  }
+  const float2 k = bc2(mx > 0.f ? FIX16_SCALE / mx : 0.f);
+  unsigned w[12];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    w[2 * c] = fix16_pack2(x.up.re[c], k);
+    w[2 * c + 1] = fix16_pack2(x.up.im[c], k);
+    w[6 + 2 * c] = fix16_pack2(x.lo.re[c], k);
+    w[6 + 2 * c + 1] = fix16_pack2(x.lo.im[c], k);
+  }
+  uint4 *p = static_cast<uint4 *>(v.p) + blk_base<3>(s);
+#pragma unroll
+  for (int j = 0; j < 3; j++) p[j * SB] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
+  v.norm[s] = mx;
+}
+
+// a site of an FP32 (SOA32) or 16-bit (SOA16) field as lane pairs, in value units
+template <int K>
+__device__ __forceinline__ void site_load2(const SpinorView<K> &v, int s, Site2 &o) {
+  if constexpr (K == SOA32) {
+    site2_load(v, s, o);
+  } else {
+    static_assert(K == SOA16, "paired site I/O: SOA32 or SOA16");
+    const float nrm = site16_load_raw(v, s, o);
+    site2_scale(o, bc2(nrm * (1.0f / FIX16_SCALE)));
+  }
+}
+template <int K>
+__device__ __forceinline__ void site_store2(const SpinorView<K> &v, int s, const Site2 &w) {
+  if constexpr (K == SOA32) site2_store(v, s, w);
+  else site16_store(v, s, w);
+}
+
 // ------------------------------------------------------------------ links
 // row 2 = conj(row0 x row1), on broadcast pairs (k = 3 * r + c)
 __device__ __forceinline__ void link2_row2(Link2 &m) {
@@ -168,10 +247,11 @@ __device__ __forceinline__ float link2_load(const GaugeView<G> &u, int dir, int 
 }
 
 // ------------------------------------------------------------------ one hop
-// acc += U (1 - gamma_mu) psi (FWD) or U^dag (1 + gamma_mu) psi (!FWD), times
-// ph (the time-boundary phase; 1 for mu < 3).  Gamma conventions as gcol /
-// gre / gim in fields.cuh.
-template <int MU, bool FWD>
+// acc += f U (1 - gamma_mu) psi (FWD) or f U^dag (1 + gamma_mu) psi (!FWD).
+// f (the time-boundary phase, times the neighbour's norm for 16-bit spinors)
+// scales the projected half spinor; it is taken as 1 unless MU == 3 or
+// SCALED.  Gamma conventions as gcol / gre / gim in fields.cuh.
+template <int MU, bool FWD, bool SCALED>
 __device__ __forceinline__ void hop2(Site2 &acc, const Site2 &psi, const Link2 &u, float ph) {
   constexpr int S = FWD ? -1 : 1;
   SpinPair h, uh;
@@ -197,7 +277,7 @@ __device__ __forceinline__ void hop2(Site2 &acc, const Site2 &psi, const Link2 &
       h.im[c] = make_float2(psi.up.im[c].x + q0.im, psi.up.im[c].y + q1.im);
     }
   }
-  if constexpr (MU == 3) {
+  if constexpr (MU == 3 || SCALED) {
     const float2 f = bc2(ph);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -268,23 +348,24 @@ __device__ __forceinline__ void hop2(Site2 &acc, const Site2 &psi, const Link2 &
   }
 }
 
-template <int MU, bool FWD, int G>
-__device__ __forceinline__ float hop2_from(Site2 &acc, const SpinorView<SOA32> &in, const GaugeView<G> &U, int n,
+template <int MU, bool FWD, int K, int G>
+__device__ __forceinline__ float hop2_from(Site2 &acc, const SpinorView<K> &in, const GaugeView<G> &U, int n,
                                            int lpar, int ls, float ph) {
   Site2 psi;
   Link2 u;
-  site2_load(in, n, psi);
+  if constexpr (K == SOA16) ph *= site16_load_raw(in, n, psi) * (1.0f / FIX16_SCALE);
+  else site2_load(in, n, psi);
   const float unit = link2_load<G>(U, MU, lpar, ls, u);
-  hop2<MU, FWD>(acc, psi, u, ph);
+  hop2<MU, FWD, K == SOA16>(acc, psi, u, ph);
   return unit;
 }
 
-// Hopping term D_{p <- 1-p} at output site s of parity par, FP32 spinors:
+// Hopping term D_{p <- 1-p} at output site s of parity par, FP32 or 16-bit spinors:
 // acc = the sum over the eight hops in units of the returned value (1/32767
 // for 16-bit links, 1 for FP32 links), which the caller folds into its own
 // scale factor.  Neighbour indexing as wilson_hop_site.
-template <int G>
-__device__ __forceinline__ float wilson_hop_site2(Site2 &acc, const SpinorView<SOA32> &in, const GaugeView<G> &U,
+template <int K, int G>
+__device__ __forceinline__ float wilson_hop_site2(Site2 &acc, const SpinorView<K> &in, const GaugeView<G> &U,
                                                   const Geom &g, int s, int par, float t_bc) {
 #pragma unroll
   for (int c = 0; c < 3; c++) {
