@@ -186,21 +186,18 @@ __device__ __forceinline__ void site_store2(const SpinorView<K> &v, int s, const
 }
 
 // ------------------------------------------------------------------ links
-// row 2 = conj(row0 x row1), on broadcast pairs (k = 3 * r + c)
-__device__ __forceinline__ void link2_row2(Link2 &m) {
+// row 2 = conj(row0 x row1) times f, computed once in scalar FP32 (a paired
+// instruction takes the FMA pipe for two lanes, so a broadcast pair would
+// cost twice) and then broadcast (k = 3 * r + c)
+__device__ __forceinline__ void link2_row2(Link2 &m, float f) {
+  Cpx<float> r[9];
+#pragma unroll
+  for (int k = 0; k < 6; k++) r[k] = Cpx<float>(m.re[k].x, m.im[k].x);
+  su3_row2(r);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    const int a = (c + 1) % 3, b = (c + 2) % 3;  // m[2][c] = conj(m0a m1b - m0b m1a)
-    float2 re = mul2(m.re[a], m.re[3 + b]);
-    re = fma2(neg2(m.im[a]), m.im[3 + b], re);
-    re = fma2(neg2(m.re[b]), m.re[3 + a], re);
-    re = fma2(m.im[b], m.im[3 + a], re);
-    float2 im = mul2(neg2(m.re[a]), m.im[3 + b]);
-    im = fma2(neg2(m.im[a]), m.re[3 + b], im);
-    im = fma2(m.re[b], m.im[3 + a], im);
-    im = fma2(m.im[b], m.re[3 + a], im);
-    m.re[6 + c] = re;
-    m.im[6 + c] = im;
+    m.re[6 + c] = bc2(r[6 + c].re * f);
+    m.im[6 + c] = bc2(r[6 + c].im * f);
   }
 }
 
@@ -221,7 +218,7 @@ __device__ __forceinline__ float link2_load(const GaugeView<G> &u, int dir, int 
       m.re[2 * k + 1] = bc2(d.z);
       m.im[2 * k + 1] = bc2(d.w);
     }
-    link2_row2(m);
+    link2_row2(m, 1.0f);
     return 1.0f;
   } else {
     static_assert(G == GSOA16, "FP32 hop: GSOA32 or GSOA16 links");
@@ -235,13 +232,7 @@ __device__ __forceinline__ float link2_load(const GaugeView<G> &u, int dir, int 
       m.re[2 * k + 1] = bc2(b.x);
       m.im[2 * k + 1] = bc2(b.y);
     }
-    link2_row2(m);
-    const float2 unit = bc2(1.0f / FIX16_SCALE);
-#pragma unroll
-    for (int k = 6; k < 9; k++) {
-      m.re[k] = mul2(m.re[k], unit);
-      m.im[k] = mul2(m.im[k], unit);
-    }
+    link2_row2(m, 1.0f / FIX16_SCALE);
     return 1.0f / FIX16_SCALE;
   }
 }
