@@ -17,22 +17,27 @@
 
 namespace qcu {
 
-// resident blocks per SM requested from the register allocator: the FP64
-// kernels would otherwise take ~176 registers (2 blocks of 128 threads per SM);
-// 3 blocks fit in 170 registers without spills.  The variants with a reduction
-// stride over the sites with one resident wave of 3 blocks per SM (forcing the
-// 16/32-bit ones to 128 registers for a 4th block measured slower).
-// The FP32- and 16-bit-spinor kernels (paired FP32 instructions, hop32.cuh)
-// issue few enough instructions to be bound by memory latency instead: they
-// take more resident blocks (72 registers, 7 blocks of 128 threads) for more
-// loads in flight.
+// Resident blocks per SM requested from the register allocator.  The FP64
+// kernels would otherwise take ~176 registers (2 blocks of 128 threads per
+// SM); 3 blocks fit in 170 registers without spills.  The FP32- and
+// 16-bit-spinor kernels (paired FP32 instructions, hop32.cuh) issue few
+// enough instructions to be bound by memory latency instead: they take more
+// resident blocks (72 registers, 7 blocks) for more loads in flight.  The
+// variants with a reduction stride over the sites with one resident wave of 3
+// blocks per SM, except the 16-bit ones (below).
 #ifndef QCU_DSLASH32_BLOCKS
 #define QCU_DSLASH32_BLOCKS 7  // FP32 / 16-bit spinors without a reduction
 #endif
-#ifndef QCU_DSLASH32_RED_BLOCKS
-#define QCU_DSLASH32_RED_BLOCKS 3  // FP32 / 16-bit spinors with a reduction
+#ifndef QCU_DSLASH16_RED_BLOCKS
+#define QCU_DSLASH16_RED_BLOCKS 6  // 16-bit spinors with a reduction
 #endif
-#define DSLASH_RED_BLOCKS(K) (((K) == SOA32 || (K) == SOA16) ? QCU_DSLASH32_RED_BLOCKS : 3)
+// 16-bit spinors reduce in two kernels: every block of the dslash writes its
+// partial, and a one-block kernel sums them.  The strided one-wave form
+// (every other kind) takes ~165 registers there and 3 resident blocks; the
+// split form fits 80 registers and 6 blocks, which measured faster for the
+// 16-bit kernels and slower for the FP32 ones.
+#define DSLASH_SPLIT_RED(K) ((K) == SOA16)
+#define DSLASH_RED_BLOCKS(K) ((K) == SOA16 ? QCU_DSLASH16_RED_BLOCKS : 3)
 #define DSLASH_MIN_BLOCKS(K, RED) \
   (((K) == AOS64 || (K) == SOA64) ? 3 : ((RED) == RED_NONE ? QCU_DSLASH32_BLOCKS : DSLASH_RED_BLOCKS(K)))
 
@@ -142,6 +147,17 @@ __global__ void __launch_bounds__(DSLASH_BLOCK, DSLASH_MIN_BLOCKS(K, RED)) k_dsl
   if constexpr (RED == RED_NONE) {
     const int s = blockIdx.x * DSLASH_BLOCK + threadIdx.x;  // one site per thread
     if (s < g.Vh) dslash_site<K, G, C, CLOV, NX, RED, NV>(g, a, s, red);
+  } else if constexpr (DSLASH_SPLIT_RED(K)) {
+    // one site per thread; the block's partial goes to partials[k * grid + b]
+    // and k_red_finish, launched next, reduces them
+    const int s = blockIdx.x * DSLASH_BLOCK + threadIdx.x;
+    if (s < g.Vh) dslash_site<K, G, C, CLOV, NX, RED, NV>(g, a, s, red);
+    double part[NV];
+    block_sum<NV, DSLASH_BLOCK>(red, part);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < NV; k++) rc.partials[(size_t)k * gridDim.x + blockIdx.x] = part[k];
+    }
   } else {
     // a grid of resident blocks strides over the sites, so the block
     // reduction and the ticket (barriers, a fence, an atomic) are paid once
@@ -152,11 +168,28 @@ __global__ void __launch_bounds__(DSLASH_BLOCK, DSLASH_MIN_BLOCKS(K, RED)) k_dsl
   }
 }
 
+// Sum of the n block partials of a split reduction, in block order, and the
+// finalize op; skipped with the dslash it belongs to when its gate is closed.
+constexpr int FINISH_BLOCK = 512;
+template <int NV>
+__global__ void __launch_bounds__(FINISH_BLOCK) k_red_finish(const double *partials, int n, SolverState *st, int op,
+                                                           int gate) {
+  if (!gate_open(st, gate)) return;
+  double tot[NV];
+  sum_partials<NV, FINISH_BLOCK>(partials, n, tot);
+  if (threadIdx.x == 0) {
+    double v[RED_MAXV];
+#pragma unroll
+    for (int k = 0; k < RED_MAXV; k++) v[k] = k < NV ? tot[k] : 0.0;
+    finalize(st, op, v);
+  }
+}
+
 template <int K, int G, int C, bool CLOV, int NX, int RED>
 static void launch_t(const Geom &g, const DslashArgs &a, Context &ctx, cudaStream_t s) {
   int blocks = (g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK;
   // reductions: one resident wave (the 16/32-bit reducing variants take ~167 registers, FP64 170)
-  if (RED != RED_NONE) blocks = std::min(blocks, DSLASH_RED_BLOCKS(K) * ctx.sms);
+  if (RED != RED_NONE && !DSLASH_SPLIT_RED(K)) blocks = std::min(blocks, DSLASH_RED_BLOCKS(K) * ctx.sms);
   RedCtx rc{ctx.st, ctx.partials, a.fin};
   if (RED != RED_NONE) {
     require(a.gate == GATE_ALWAYS || ctx.st != nullptr, "reduction without solver state");
@@ -165,6 +198,11 @@ static void launch_t(const Geom &g, const DslashArgs &a, Context &ctx, cudaStrea
   }
   k_dslash<K, G, C, CLOV, NX, RED><<<blocks, DSLASH_BLOCK, 0, s>>>(g, a, rc);
   QCU_CHECK_LAUNCH();
+  if (RED != RED_NONE && DSLASH_SPLIT_RED(K)) {
+    constexpr int NV = RED == RED_TS_TT ? 3 : (RED == RED_DOT_RT ? 2 : 1);
+    k_red_finish<NV><<<1, FINISH_BLOCK, 0, s>>>(rc.partials, blocks, rc.st, rc.op, a.gate);
+    QCU_CHECK_LAUNCH();
+  }
 }
 
 template <int K, int G, int C, bool CLOV>
