@@ -9,8 +9,10 @@
 // last block of the rhs's own tiles (per-rhs ticket, fixed summation order,
 // so results are deterministic and independent of the other rhs).
 #include <algorithm>
+#include <type_traits>
 
 #include "batch_dev.cuh"
+#include "hop32.cuh"
 
 namespace qcu {
 
@@ -80,10 +82,70 @@ __device__ __forceinline__ void wilson_hop_group(Cpx<T> (&acc)[NR][12], const Sp
   hop_group<3, false>(acc, in, on, U, n, 1 - par, n, (t == 0) ? t_bc : T(1));
 }
 
-// resident blocks asked of the register allocator: 4 x 128 threads (128
-// registers) for one FP32 rhs per thread, 3 x 128 for FP64; the
+// FP32 spinors: the same hops on spin-paired registers (hop32.cuh), each
+// link decoded and broadcast once for the NR right-hand sides.  acc holds the
+// hop sums in units of the returned value (1/32767 for 16-bit links).
+template <int G, int NR>
+__device__ __forceinline__ float wilson_hop_group2(Site2 (&acc)[NR], const SpinorView<SOA32> (&in)[NR],
+                                                   const GaugeView<G> &U, const Geom &g, int s, int par, float t_bc) {
+#pragma unroll
+  for (int j = 0; j < NR; j++)
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      acc[j].up.re[c] = acc[j].up.im[c] = acc[j].lo.re[c] = acc[j].lo.im[c] = make_float2(0.f, 0.f);
+  const int xh = s % g.Lxh;
+  int r = s / g.Lxh;
+  const int y = r % g.Ly;
+  r /= g.Ly;
+  const int z = r % g.Lz;
+  const int t = r / g.Lz;
+  const int xodd = (y + z + t + par) & 1;
+  float unit = 1.0f;
+  auto hop = [&](auto mu_c, auto fwd_c, int n, int lpar, int ls, float ph) {
+    constexpr int MU = decltype(mu_c)::value;
+    constexpr bool FWD = decltype(fwd_c)::value;
+    Link2 u;
+    unit = link2_load<G>(U, MU, lpar, ls, u);
+#pragma unroll
+    for (int j = 0; j < NR; j++) {  // every slot is computed; closed slots read a valid buffer
+      Site2 psi;
+      site2_load(in[j], n, psi);
+      hop2<MU, FWD, false>(acc[j], psi, u, ph);
+    }
+  };
+  using I0 = std::integral_constant<int, 0>;
+  using I1 = std::integral_constant<int, 1>;
+  using I2 = std::integral_constant<int, 2>;
+  using I3 = std::integral_constant<int, 3>;
+  using BT = std::true_type;
+  using BF = std::false_type;
+  int n;
+  n = xodd ? (xh == g.Lxh - 1 ? s - xh : s + 1) : s;
+  hop(I0{}, BT{}, n, par, s, 1.f);
+  n = xodd ? s : (xh == 0 ? s + g.Lxh - 1 : s - 1);
+  hop(I0{}, BF{}, n, 1 - par, n, 1.f);
+  n = (y == g.Ly - 1) ? s - (g.Ly - 1) * g.sy : s + g.sy;
+  hop(I1{}, BT{}, n, par, s, 1.f);
+  n = (y == 0) ? s + (g.Ly - 1) * g.sy : s - g.sy;
+  hop(I1{}, BF{}, n, 1 - par, n, 1.f);
+  n = (z == g.Lz - 1) ? s - (g.Lz - 1) * g.sz : s + g.sz;
+  hop(I2{}, BT{}, n, par, s, 1.f);
+  n = (z == 0) ? s + (g.Lz - 1) * g.sz : s - g.sz;
+  hop(I2{}, BF{}, n, 1 - par, n, 1.f);
+  n = (t == g.Lt - 1) ? s - (g.Lt - 1) * g.st : s + g.st;
+  hop(I3{}, BT{}, n, par, s, (t == g.Lt - 1) ? t_bc : 1.f);
+  n = (t == 0) ? s + (g.Lt - 1) * g.st : s - g.st;
+  hop(I3{}, BF{}, n, 1 - par, n, (t == 0) ? t_bc : 1.f);
+  return unit;
+}
+
+// resident blocks asked of the register allocator: QCU_BDSL32_BLOCKS x 128
+// threads for one FP32 rhs per thread, 3 x 128 for FP64; the
 // register-blocked groups keep their registers
-#define BDSL_MIN_BLOCKS(K, NT, NR) ((K) == SOA64 ? 384 / (NT) : ((NR) == 1 ? 512 / (NT) : 1))
+#ifndef QCU_BDSL32_BLOCKS
+#define QCU_BDSL32_BLOCKS 4
+#endif
+#define BDSL_MIN_BLOCKS(K, NT, NR) ((K) == SOA64 ? 384 / (NT) : ((NR) == 1 ? QCU_BDSL32_BLOCKS * 128 / (NT) : 1))
 
 // Tile = (group of NR rhs of one system, block of NT sites); every thread
 // computes its site for all open rhs of the group, then the epilogue and the
@@ -117,9 +179,17 @@ __device__ __forceinline__ void kb_dslash_tile(const BatchArgs &a, const int2 ti
 #pragma unroll
     for (int j = 0; j < NR; j++) in[j] = bview<K>(a.d[grp.rhs[j]], op.in);  // empty slots repeat the first rhs
     const GaugeView<G> U{K == SOA64 ? d0.g64 : d0.gin, pad_sites(g.Vh)};
-    wilson_hop_group<K, G, T, NR>(w, in, on, U, g, s, op.parity, (T)d0.t_bc);
+    T unit = T(1);
+    if constexpr (K == SOA32) {
+      Site2 w2[NR];
+      unit = wilson_hop_group2<G, NR>(w2, in, U, g, s, op.parity, (float)d0.t_bc);
+#pragma unroll
+      for (int j = 0; j < NR; j++) site2_to_cpx(w2[j], w[j]);
+    } else {
+      wilson_hop_group<K, G, T, NR>(w, in, on, U, g, s, op.parity, (T)d0.t_bc);
+    }
     const void *cl = CLOV ? (K == SOA64 ? d0.c64[op.parity] : d0.cin[op.parity]) : nullptr;
-    const T aa = (T)(op.a0 + op.ak * d0.kappa + op.ak2 * d0.k2);
+    const T aa = (T)(op.a0 + op.ak * d0.kappa + op.ak2 * d0.k2) * unit;
 #pragma unroll
     for (int j = 0; j < NR; j++) {
       if (!on[j]) continue;
