@@ -46,6 +46,28 @@ __device__ __forceinline__ float2 fmak(float2 a, float2 c) {
   else return fma2(a, make_float2((float)K0, (float)K1), c);
 }
 
+constexpr float K16 = 8421376.0f;  // 2^23 + 32768: offset of a biased 16-bit value
+
+// The same on biased inputs a = K16 + v_a, c = K16 + v_c (16-bit spinors):
+// returns v_c + k v_a exactly.  A lane with k = -1 needs nothing (the offsets
+// cancel in c - a); a lane with k = +1 first takes 2 K16 off c.  Every step is
+// exact: the operands are integers below 2^24 and the sums cancel to |v| <= 65534.
+template <int K0, int K1>
+__device__ __forceinline__ float2 fmak_biased(float2 a, float2 c) {
+  if constexpr (K0 == 1 || K1 == 1)
+    c = add2(c, make_float2(K0 == 1 ? -2.0f * K16 : 0.0f, K1 == 1 ? -2.0f * K16 : 0.0f));
+  return fmak<K0, K1>(a, c);
+}
+// scalar form: v_a + q, where q is a biased value times the unit SG (+1 or -1)
+template <int SG>
+__device__ __forceinline__ float comb_biased(float ra, float q) {
+  if constexpr (SG > 0) return (ra - 2.0f * K16) + q;
+  else return ra + q;
+}
+// sign (+1/-1) of the real and imaginary component of unit_mul<RE, IM>(z) relative to z's components
+__host__ __device__ constexpr int unit_sign_re(int re, int im) { return re != 0 ? re : -im; }
+__host__ __device__ constexpr int unit_sign_im(int re, int im) { return re != 0 ? re : im; }
+
 // ------------------------------------------------------------------ SOA32 site I/O
 __device__ __forceinline__ void site2_load(const SpinorView<SOA32> &v, int s, Site2 &o) {
   const float4 *p = static_cast<const float4 *>(v.p) + blk_base<6>(s);
@@ -136,6 +158,35 @@ __device__ __forceinline__ float site16_load_raw(const SpinorView<SOA16> &v, int
     o.up.im[c] = fix16_unpack2(w[2 * c + 1]);
     o.lo.re[c] = fix16_unpack2(w[6 + 2 * c]);
     o.lo.im[c] = fix16_unpack2(w[6 + 2 * c + 1]);
+  }
+  return __ldg(v.norm + s);
+}
+
+// The same site with the decode's offset left in: every value is r = K16 + v
+// (K16 = 2^23 + 32768, v the integer value), exactly as the byte permute
+// makes it.  The projection of a hop removes the offset itself (hop2), in
+// fewer operations than decoding each value first.
+__device__ __forceinline__ float2 fix16_biased2(unsigned w) {
+  return make_float2(__int_as_float(__byte_perm(w, 0x4B000000u, 0x7610)),
+                     __int_as_float(__byte_perm(w, 0x4B000000u, 0x7632)));
+}
+__device__ __forceinline__ float site16_load_biased(const SpinorView<SOA16> &v, int s, Site2 &o) {
+  const uint4 *p = static_cast<const uint4 *>(v.p) + blk_base<3>(s);
+  unsigned w[12];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const uint4 d = __ldg(p + j * SB);
+    w[4 * j] = d.x;
+    w[4 * j + 1] = d.y;
+    w[4 * j + 2] = d.z;
+    w[4 * j + 3] = d.w;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    o.up.re[c] = fix16_biased2(w[2 * c]);
+    o.up.im[c] = fix16_biased2(w[2 * c + 1]);
+    o.lo.re[c] = fix16_biased2(w[6 + 2 * c]);
+    o.lo.im[c] = fix16_biased2(w[6 + 2 * c + 1]);
   }
   return __ldg(v.norm + s);
 }
@@ -242,7 +293,9 @@ __device__ __forceinline__ float link2_load(const GaugeView<G> &u, int dir, int 
 // f (the time-boundary phase, times the neighbour's norm for 16-bit spinors)
 // scales the projected half spinor; it is taken as 1 unless MU == 3 or
 // SCALED.  Gamma conventions as gcol / gre / gim in fields.cuh.
-template <int MU, bool FWD, bool SCALED>
+// BIASED: psi holds the biased values of a 16-bit spinor (site16_load_biased);
+// the projection returns exact values all the same.
+template <int MU, bool FWD, bool SCALED, bool BIASED = false>
 __device__ __forceinline__ void hop2(Site2 &acc, const Site2 &psi, const Link2 &u, float ph) {
   constexpr int S = FWD ? -1 : 1;
   SpinPair h, uh;
@@ -251,7 +304,15 @@ __device__ __forceinline__ void hop2(Site2 &acc, const Site2 &psi, const Link2 &
     constexpr int A0 = S * gre(MU, 0), A1 = S * gre(MU, 1), B0 = S * gim(MU, 0), B1 = S * gim(MU, 1);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      if constexpr (A0 != 0) {
+      if constexpr (BIASED) {
+        if constexpr (A0 != 0) {
+          h.re[c] = fmak_biased<A0, A1>(psi.lo.re[c], psi.up.re[c]);
+          h.im[c] = fmak_biased<A0, A1>(psi.lo.im[c], psi.up.im[c]);
+        } else {
+          h.re[c] = fmak_biased<-B0, -B1>(psi.lo.im[c], psi.up.re[c]);
+          h.im[c] = fmak_biased<B0, B1>(psi.lo.re[c], psi.up.im[c]);
+        }
+      } else if constexpr (A0 != 0) {
         h.re[c] = fmak<A0, A1>(psi.lo.re[c], psi.up.re[c]);
         h.im[c] = fmak<A0, A1>(psi.lo.im[c], psi.up.im[c]);
       } else {
@@ -262,10 +323,18 @@ __device__ __forceinline__ void hop2(Site2 &acc, const Site2 &psi, const Link2 &
   } else {  // gcol = 3, 2: crossed lanes, scalar
 #pragma unroll
     for (int c = 0; c < 3; c++) {  // h_0 from spin 3 (lane y), h_1 from spin 2 (lane x)
-      const Cpx<float> q0 = unit_mul<S * gre(MU, 0), S * gim(MU, 0)>(Cpx<float>(psi.lo.re[c].y, psi.lo.im[c].y));
-      const Cpx<float> q1 = unit_mul<S * gre(MU, 1), S * gim(MU, 1)>(Cpx<float>(psi.lo.re[c].x, psi.lo.im[c].x));
-      h.re[c] = make_float2(psi.up.re[c].x + q0.re, psi.up.re[c].y + q1.re);
-      h.im[c] = make_float2(psi.up.im[c].x + q0.im, psi.up.im[c].y + q1.im);
+      constexpr int R0 = S * gre(MU, 0), I0 = S * gim(MU, 0), R1 = S * gre(MU, 1), I1 = S * gim(MU, 1);
+      const Cpx<float> q0 = unit_mul<R0, I0>(Cpx<float>(psi.lo.re[c].y, psi.lo.im[c].y));
+      const Cpx<float> q1 = unit_mul<R1, I1>(Cpx<float>(psi.lo.re[c].x, psi.lo.im[c].x));
+      if constexpr (BIASED) {
+        h.re[c] = make_float2(comb_biased<unit_sign_re(R0, I0)>(psi.up.re[c].x, q0.re),
+                              comb_biased<unit_sign_re(R1, I1)>(psi.up.re[c].y, q1.re));
+        h.im[c] = make_float2(comb_biased<unit_sign_im(R0, I0)>(psi.up.im[c].x, q0.im),
+                              comb_biased<unit_sign_im(R1, I1)>(psi.up.im[c].y, q1.im));
+      } else {
+        h.re[c] = make_float2(psi.up.re[c].x + q0.re, psi.up.re[c].y + q1.re);
+        h.im[c] = make_float2(psi.up.im[c].x + q0.im, psi.up.im[c].y + q1.im);
+      }
     }
   }
   if constexpr (MU == 3 || SCALED) {
@@ -344,10 +413,10 @@ __device__ __forceinline__ float hop2_from(Site2 &acc, const SpinorView<K> &in, 
                                            int lpar, int ls, float ph) {
   Site2 psi;
   Link2 u;
-  if constexpr (K == SOA16) ph *= site16_load_raw(in, n, psi) * (1.0f / FIX16_SCALE);
+  if constexpr (K == SOA16) ph *= site16_load_biased(in, n, psi) * (1.0f / FIX16_SCALE);
   else site2_load(in, n, psi);
   const float unit = link2_load<G>(U, MU, lpar, ls, u);
-  hop2<MU, FWD, K == SOA16>(acc, psi, u, ph);
+  hop2<MU, FWD, K == SOA16, K == SOA16>(acc, psi, u, ph);
   return unit;
 }
 
