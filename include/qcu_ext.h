@@ -41,7 +41,8 @@ int qcuGaugeFree(qcuGauge h);
 
 /* half spinors: out(parity) = [A_parity^{-1}] D_{parity <- 1-parity} in, computed
  * with the field stored in `precision` bits (64, 32, or 16 = int16 fixed point + per-site
- * norm; accumulation in FP64 resp. FP32); input and output stay complex128 */
+ * norm; accumulation in FP64 resp. FP32), or 3216 = FP32 spinors with 16-bit links;
+ * input and output stay complex128 */
 int qcuDslash(qcuGauge h, void *out, const void *in, int parity, int use_clover, int precision);
 /* odd-parity Schur operator M_pc = 1 - kappa^2 [A_o^-1] D_oe [A_e^-1] D_eo */
 int qcuMatPC(qcuGauge h, void *out, const void *in, double kappa, int use_clover);

@@ -267,6 +267,9 @@ class Gauge:
         self.close()
 
     def dslash(self, out, inp, parity: int, clover: bool = False, precision: int = 64):
+        """out = [A^-1] D in on PyQuda-layout half spinors, computed with the
+        spinors stored in `precision` bits (64, 32, 16) or as FP32 spinors
+        with 16-bit links (3216)."""
         _check(_lib.qcuDslash(self._h, _ptr(out), _ptr(inp), int(parity), int(clover), int(precision)))
 
     def matpc(self, out, inp, kappa: float, clover: bool = False):

@@ -618,7 +618,8 @@ void handle_dslash(GaugeHandle &G, void *out, const void *in, int par, int use_c
   require(out && in, "dslash: null spinor pointer");
   require(par == 0 || par == 1, "parity must be 0 or 1");
   require(!use_clover || G.has_clover, "dslash: no clover term loaded");
-  const int kind = kind_of_precision(precision);
+  const bool links16 = precision == 3216;  // FP32 spinors with 16-bit links (the FP32 inner operator)
+  const int kind = kind_of_precision(links16 ? 32 : precision);
   Context &ctx = context();
   std::lock_guard<std::mutex> lk(ctx.mu);
   Workspace &w = workspace();
@@ -629,7 +630,7 @@ void handle_dslash(GaugeHandle &G, void *out, const void *in, int par, int use_c
   w.tmp.alloc(kind, Vh);
   Spinor &a = kind == SOA64 ? w.aux : w.r, &b = kind == SOA64 ? w.tmp64 : w.tmp;
   QCU_CUDA(cudaDeviceSynchronize());
-  Dsl d{G, ctx, kind};
+  Dsl d{G, ctx, kind, links16 ? GSOA16 : -1};
   launch_convert(AOS64, kind, Vh, in, nullptr, a.data.p, a.norm.as<float>(), ctx.stream);
   d(par, a, b, use_clover != 0, 1.0);
   launch_convert(kind, AOS64, Vh, b.data.p, b.norm.as<float>(), out, nullptr, ctx.stream);

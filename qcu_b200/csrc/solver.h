@@ -84,7 +84,8 @@ double finish_solution(Dsl &d64, double kappa, bool clov, Spinor &be, Spinor &bo
                        Spinor &aux, Spinor &tmp64, void *x_pyq);
 
 // out = D_{par <- 1-par} in on PyQuda-layout half spinors (optionally A^-1 D),
-// computed in the given storage precision (64, 32, 16) on the packed gauge
+// computed in the given storage precision (64, 32, 16; 3216 = FP32 spinors with
+// 16-bit links) on the packed gauge
 void handle_dslash(GaugeHandle &G, void *out, const void *in, int par, int use_clover, int precision);
 // out = M_pc in (odd parity, PyQuda-layout half spinors)
 void handle_mpc(GaugeHandle &G, void *out, const void *in, double kappa, int use_clover);

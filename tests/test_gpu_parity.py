@@ -80,10 +80,12 @@ def test_dslashCloverQcu(q, latt, kind):
         assert rel(host(out), expect) <= 1e-14 * max(cond, 10)
 
 
+@pytest.mark.parametrize("latt", [[8, 4, 6, 8], [6, 2, 2, 6]])  # Vh = 768 and 72 (not a multiple of 32)
 @pytest.mark.parametrize("t_bc", [1.0, -1.0])
-@pytest.mark.parametrize("prec,tol", [(64, 1e-13), (32, 1e-6), (16, 2e-4)])
-def test_ext_dslash_precisions(q, t_bc, prec, tol):
-    latt = [8, 4, 6, 8]
+@pytest.mark.parametrize("prec,tol", [(64, 1e-13), (32, 1e-6), (16, 2e-4), (3216, 2e-4)])
+def test_ext_dslash_precisions(q, latt, t_bc, prec, tol):
+    """Every storage precision of the hopping term against the FP64 oracle
+    (3216: FP32 spinors with 16-bit links)."""
     U, psi = _fields(latt, "smooth", 5)
     with q.Gauge(dev(U), latt, t_boundary=t_bc) as G:
         for p in (0, 1):
@@ -92,7 +94,7 @@ def test_ext_dslash_precisions(q, t_bc, prec, tol):
             assert rel(host(out), O.dslash(psi[1 - p], U, latt, p, t_bc)) <= tol
 
 
-@pytest.mark.parametrize("prec,tol", [(64, 1e-13), (32, 1e-6)])
+@pytest.mark.parametrize("prec,tol", [(64, 1e-13), (32, 1e-6), (16, 2e-4), (3216, 2e-4)])
 def test_ext_clover_dslash_csw(q, prec, tol):
     latt = [4, 4, 6, 8]
     U, psi = _fields(latt, "smooth", 6)
