@@ -109,8 +109,9 @@ typedef struct {
 
 /* Batched solve of every right-hand side of every system (at most 64 in
  * total; lattices may differ in size): flexible GCR(gcr_k) in FP64 per
- * right-hand side around one inner BiCGSTAB (precision 32 -- with 16-bit
- * links when gauge_precision is 16 -- or 64) that advances all right-hand
+ * right-hand side around one inner BiCGSTAB (precision 16 -- 16-bit spinors
+ * and links --, 32 -- with 16-bit links when gauge_precision is 16 -- or 64)
+ * that advances all right-hand
  * sides together, one kernel launch per step for the whole batch, captured
  * as one CUDA graph.  Uses kappa/use_clover of each system (the param's are
  * ignored), tol, maxiter (inner iterations per rhs), precision,

@@ -82,11 +82,12 @@ __device__ __forceinline__ void wilson_hop_group(Cpx<T> (&acc)[NR][12], const Sp
   hop_group<3, false>(acc, in, on, U, n, 1 - par, n, (t == 0) ? t_bc : T(1));
 }
 
-// FP32 spinors: the same hops on spin-paired registers (hop32.cuh), each
-// link decoded and broadcast once for the NR right-hand sides.  acc holds the
-// hop sums in units of the returned value (1/32767 for 16-bit links).
-template <int G, int NR>
-__device__ __forceinline__ float wilson_hop_group2(Site2 (&acc)[NR], const SpinorView<SOA32> (&in)[NR],
+// FP32 and 16-bit spinors: the same hops on spin-paired registers
+// (hop32.cuh), each link decoded and broadcast once for the NR right-hand
+// sides.  acc holds the hop sums in units of the returned value (1/32767 for
+// 16-bit links).
+template <int K, int G, int NR>
+__device__ __forceinline__ float wilson_hop_group2(Site2 (&acc)[NR], const SpinorView<K> (&in)[NR],
                                                    const GaugeView<G> &U, const Geom &g, int s, int par, float t_bc) {
 #pragma unroll
   for (int j = 0; j < NR; j++)
@@ -109,8 +110,13 @@ __device__ __forceinline__ float wilson_hop_group2(Site2 (&acc)[NR], const Spino
 #pragma unroll
     for (int j = 0; j < NR; j++) {  // every slot is computed; closed slots read a valid buffer
       Site2 psi;
-      site2_load(in[j], n, psi);
-      hop2<MU, FWD, false>(acc[j], psi, u, ph);
+      if constexpr (K == SOA16) {
+        const float f = ph * site16_load_biased(in[j], n, psi) * (1.0f / FIX16_SCALE);
+        hop2<MU, FWD, true, true>(acc[j], psi, u, f);
+      } else {
+        site2_load(in[j], n, psi);
+        hop2<MU, FWD, false>(acc[j], psi, u, ph);
+      }
     }
   };
   using I0 = std::integral_constant<int, 0>;
@@ -180,9 +186,9 @@ __device__ __forceinline__ void kb_dslash_tile(const BatchArgs &a, const int2 ti
     for (int j = 0; j < NR; j++) in[j] = bview<K>(a.d[grp.rhs[j]], op.in);  // empty slots repeat the first rhs
     const GaugeView<G> U{K == SOA64 ? d0.g64 : d0.gin, pad_sites(g.Vh)};
     T unit = T(1);
-    if constexpr (K == SOA32) {
+    if constexpr (K == SOA32 || K == SOA16) {
       Site2 w2[NR];
-      unit = wilson_hop_group2<G, NR>(w2, in, U, g, s, op.parity, (float)d0.t_bc);
+      unit = wilson_hop_group2<K, G, NR>(w2, in, U, g, s, op.parity, (float)d0.t_bc);
 #pragma unroll
       for (int j = 0; j < NR; j++) site2_to_cpx(w2[j], w[j]);
     } else {
@@ -641,26 +647,31 @@ void launch_bdslash(int kind, int gkind, const BatchArgs &a, const BDslOp &op, c
   if (kind == SOA64 && gkind == GSOA64) bdsl_shape<SOA64, GSOA64>(a, op, t, s);
   else if (kind == SOA32 && gkind == GSOA32) bdsl_shape<SOA32, GSOA32>(a, op, t, s);
   else if (kind == SOA32 && gkind == GSOA16) bdsl_shape<SOA32, GSOA16>(a, op, t, s);
+  else if (kind == SOA16 && gkind == GSOA16) bdsl_shape<SOA16, GSOA16>(a, op, t, s);
   else throw Error(1, "batched dslash: unsupported storage combination");
 }
 
 void launch_bpupdate(int kind, const BatchArgs &a, cudaStream_t s) {
   if (kind == SOA64) kb_pupdate<SOA64><<<persistent_grid(a, BB), BB, 0, s>>>(a);
+  else if (kind == SOA16) kb_pupdate<SOA16><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   else kb_pupdate<SOA32><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   QCU_CHECK_LAUNCH();
 }
 void launch_bsupdate(int kind, const BatchArgs &a, cudaStream_t s) {
   if (kind == SOA64) kb_supdate<SOA64><<<persistent_grid(a, BB), BB, 0, s>>>(a);
+  else if (kind == SOA16) kb_supdate<SOA16><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   else kb_supdate<SOA32><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   QCU_CHECK_LAUNCH();
 }
 void launch_bxrupdate(int kind, const BatchArgs &a, cudaStream_t s) {
   if (kind == SOA64) kb_xrupdate<SOA64, SOA64><<<persistent_grid(a, BB), BB, 0, s>>>(a);
+  else if (kind == SOA16) kb_xrupdate<SOA16, SOA32><<<persistent_grid(a, BB), BB, 0, s>>>(a);  // x in FP32
   else kb_xrupdate<SOA32, SOA32><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   QCU_CHECK_LAUNCH();
 }
 void launch_binit(int kind, const BatchArgs &a, cudaStream_t s) {
   if (kind == SOA64) kb_init<SOA64, SOA64><<<persistent_grid(a, BB), BB, 0, s>>>(a);
+  else if (kind == SOA16) kb_init<SOA16, SOA32><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   else kb_init<SOA32, SOA32><<<persistent_grid(a, BB), BB, 0, s>>>(a);
   QCU_CHECK_LAUNCH();
 }

@@ -30,7 +30,7 @@ struct RhsGroup {
 
 // per-rhs vectors (roles); the first group is stored in the inner precision
 enum BVec {
-  BV_R = 0, BV_RT, BV_P, BV_V, BV_S, BV_T, BV_TMP, BV_X,  // inner precision (x: FP32 or FP64)
+  BV_R = 0, BV_RT, BV_P, BV_V, BV_S, BV_T, BV_TMP, BV_X,  // inner precision (x: FP32 under 16-bit spinors)
   BV_R64, BV_Z, BV_TMP64, BV_W, BV_X64, BV_BP,          // FP64
   BV_N
 };
@@ -123,7 +123,8 @@ struct BatchSystem {
 };
 
 // Flexible GCR(gcr_k) per rhs in FP64, preconditioned by a batched inner
-// BiCGSTAB (precision 32, links 32 or 16 bit) over all rhs of all systems,
+// BiCGSTAB (precision 16 with 16-bit links, 32 with 32- or 16-bit links, or
+// 64) over all rhs of all systems,
 // captured once as a CUDA graph with a device-side WHILE loop.  One SolveInfo
 // per rhs, in system order.
 std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const SolveParams &prm, BatchTune *tune_out);

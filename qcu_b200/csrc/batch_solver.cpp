@@ -82,8 +82,7 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
   require(!prm.abs_tol && prm.x0_mode == 0, "batch: relative tolerance and a zero initial guess only");
   require(prm.precond == 0, "batch: the network preconditioner is available in single solves");
   const int kind = kind_of_precision(prm.precision);
-  require(kind == SOA32 || kind == SOA64, "batch: inner precision must be 32 or 64");
-  int gkind = kind == SOA64 ? GSOA64 : GSOA32;
+  int gkind = kind == SOA64 ? GSOA64 : (kind == SOA32 ? GSOA32 : GSOA16);  // 16-bit spinors: 16-bit links
   if (prm.gauge_precision) {
     require(prm.gauge_precision == 16 && kind == SOA32, "batch: gauge_precision 16 is available with precision 32");
     gkind = GSOA16;
@@ -125,7 +124,8 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
     RhsBufs &B = *c.rhs[r];
     const int vh = s.G->g.Vh;
     Vh[r] = vh;
-    for (int k = 0; k < BV_N; k++) B.v[k].alloc(k < BV_INNER_N ? kind : SOA64, vh);
+    for (int k = 0; k < BV_N; k++)  // the inner x stays FP32 under 16-bit spinors
+      B.v[k].alloc(k >= BV_INNER_N ? SOA64 : (k == BV_X && kind == SOA16 ? SOA32 : kind), vh);
     for (int k = 0; k < m; k++) {
       B.W[k].alloc(SOA64, vh);
       B.Z[k].alloc(SOA64, vh);
@@ -182,7 +182,7 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
   key << kind << "/" << gkind;
   for (int r = 0; r < R; r++) key << ":" << Vh[r] << (rl[r].s->use_clover ? "c" : "");
   const auto found = c.tuned.find(key.str());
-  bool need_tune = found == c.tuned.end() && kind == SOA32;
+  bool need_tune = found == c.tuned.end() && kind != SOA64;
   BatchTune tune;
   if (found != c.tuned.end()) tune = found->second;
   // QCU_BATCH_TUNE="threads,rhs,blas_sites,mma" fixes the tunables (no autotuning)

@@ -35,7 +35,7 @@ def _check(sysd, xs, tol):
         assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05 * tol
 
 
-@pytest.mark.parametrize("prec,gprec", [(64, 0), (32, 0), (32, 16)])
+@pytest.mark.parametrize("prec,gprec", [(64, 0), (32, 0), (32, 16), (16, 0)])
 def test_batch_uneven_lattices(q, prec, gprec):
     systems = [_system(q, [8, 8, 8, 8], 3, 0.124, 3, False),
                _system(q, [4, 4, 8, 8], 4, 0.125, 2, True),
@@ -56,17 +56,18 @@ def test_batch_uneven_lattices(q, prec, gprec):
             s["G"].close()
 
 
-def test_batch_matches_single_solves(q):
+@pytest.mark.parametrize("prec,gprec", [(32, 16), (16, 0)])
+def test_batch_matches_single_solves(q, prec, gprec):
     """Each rhs of a batch reaches the same solution as its own single solve."""
     s = _system(q, [8, 8, 8, 16], 7, 0.126, 4, True)
     try:
         res, _ = q.invert_batch([(s["G"], s["x"], s["db"], s["kappa"], True)], tol=1e-11, maxiter=4000,
-                                precision=32, gauge_precision=16, inner_iters=24, inner_tol=0.05, gcr_k=4)
+                                precision=prec, gauge_precision=gprec, inner_iters=24, inner_tol=0.05, gcr_k=4)
         xb = host(s["x"])
         for j in range(4):
             xs = dev(np.zeros(O.full_shape(s["latt"]), complex))
-            info = s["G"].invert(xs, s["db"][j].contiguous(), s["kappa"], tol=1e-11, maxiter=4000, precision=32,
-                                 gauge_precision=16, clover=True, solver="gcr", inner_iters=24, inner_tol=0.05,
+            info = s["G"].invert(xs, s["db"][j].contiguous(), s["kappa"], tol=1e-11, maxiter=4000, precision=prec,
+                                 gauge_precision=gprec, clover=True, solver="gcr", inner_iters=24, inner_tol=0.05,
                                  gcr_k=4)
             assert info["status"] == 1 and res[j]["status"] == 1
             d = np.linalg.norm(xb[j] - host(xs)) / np.linalg.norm(host(xs))
