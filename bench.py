@@ -361,10 +361,8 @@ def batch_config(args, q, stream, chosen_kw):
     by plain FP64 BiCGSTAB (one solve per system, times nrhs)."""
     import torch
 
-    # the batched solver's inner precisions are FP32 (16-bit links) and FP64:
-    # both arms of this comparison run FP32 spinors with 16-bit links
-    kw = {k: chosen_kw[k] for k in ("inner_iters", "inner_tol", "gcr_k")}
-    kw.update(precision=32, gauge_precision=16)
+    # both arms run the chosen solver's inner precision
+    kw = {k: chosen_kw[k] for k in ("precision", "gauge_precision", "inner_iters", "inner_tol", "gcr_k")}
     systems, handles, plain, single = [], [], 0.0, 0.0
     shapes = [(LATT, "point12"), ([16, 16, 16, 32], 4), ([24, 24, 24, 48], 4), (LATT, 4)]
     try:
@@ -403,7 +401,8 @@ def batch_config(args, q, stream, chosen_kw):
             G.close()
     return {"workload": "propagator (12 point sources) 32^3x64 + 4 rhs each on 16^3x32, 24^3x48, 32^3x64; "
                         f"clover csw {CSW}, kappa {KAPPA_CLOVER}",
-            "inner": "FP32 spinors / 16-bit links (both arms)",
+            "inner": ({16: "16-bit spinors and links", 32: "FP32 spinors", 64: "FP64"}[kw["precision"]]
+                      + (" / 16-bit links" if kw["gauge_precision"] == 16 else "") + " (both arms)"),
             "rhs": len(res), "seconds": round(tb, 4), "tune": tune,
             "iterations_max": max(r["iterations"] for r in res),
             "max_true_residual": max(r["true_residual"] for r in res),
