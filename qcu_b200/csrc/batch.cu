@@ -17,25 +17,18 @@
 namespace qcu {
 
 // ---------------------------------------------------------------- hopping term
-// One hop for the NR right-hand sides of a group: the link is loaded (and
-// for 16-bit links decoded and row 2 rebuilt) once, scaled once, and applied
-// to each right-hand side's neighbour spinor.
+// One FP64 hop for the NR right-hand sides of a group: the link is loaded
+// (row 2 rebuilt) once, scaled once, and applied to each right-hand side's
+// neighbour spinor.  (FP32 and 16-bit spinors: wilson_hop_group2 below.)
 template <int MU, bool FWD, int K, int G, typename T, int NR>
 __device__ __forceinline__ void hop_group(Cpx<T> (&acc)[NR][12], const SpinorView<K> (&in)[NR], const bool (&on)[NR],
                                           const GaugeView<G> &U, int n, int lpar, int ls, T ph) {
+  static_assert(K == SOA64, "the scalar group hop is the FP64 one");
   Cpx<T> u[9];
-  if constexpr (K == SOA32 && G == GSOA16) {
-    Cpx<float> uf[9];
-    link16_load_raw(U, MU, lpar, ls, uf);
-    const float f = (1.0f / FIX16_SCALE) * (float)ph;
+  link_load<G, T>(U, MU, lpar, ls, u);
+  if constexpr (MU == 3) {
 #pragma unroll
-    for (int k = 0; k < 9; k++) u[k] = uf[k] * f;
-  } else {
-    link_load<G, T>(U, MU, lpar, ls, u);
-    if constexpr (MU == 3) {
-#pragma unroll
-      for (int k = 0; k < 9; k++) u[k] = u[k] * ph;
-    }
+    for (int k = 0; k < 9; k++) u[k] = u[k] * ph;
   }
   // every slot is computed (a closed or empty slot reads a valid buffer and
   // is discarded in the epilogue): no branch between the loads of the slots

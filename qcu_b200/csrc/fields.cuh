@@ -234,23 +234,6 @@ __device__ __forceinline__ void link_load(const GaugeView<G> &u, int dir, int pa
   m[8] = (m[0] * m[4] - m[1] * m[3]).conj();
 }
 
-// GSOA16 link in units of 1/32767 (rows 0-1 as stored; row 2 rebuilt and
-// brought to the same units by one factor 1/32767)
-__device__ __forceinline__ void link16_load_raw(const GaugeView<GSOA16> &u, int dir, int par, int s, Cpx<float> m[9]) {
-  const size_t slab = (size_t)(dir * 2 + par) * u.stride;
-  const uint2 *p = static_cast<const uint2 *>(u.p) + slab * 3 + blk_base<3>(s);
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    uint2 d = __ldg(p + k * SB);
-    const float2 a = fix16_unpack(d.x), b = fix16_unpack(d.y);
-    m[2 * k] = Cpx<float>(a.x, a.y);
-    m[2 * k + 1] = Cpx<float>(b.x, b.y);
-  }
-  su3_row2(m);
-#pragma unroll
-  for (int k = 6; k < 9; k++) m[k] = m[k] * (1.0f / FIX16_SCALE);
-}
-
 // ------------------------------------------------------------------ stencil
 // DeGrand-Rossi gamma matrices: row r of gamma_mu has one non-zero entry, in
 // column GCOL[mu][r], with value GRE + i*GIM.  These are the projections qcu
