@@ -80,6 +80,8 @@ typedef struct {
   double true_residual;  /* ||b - M x|| / ||b||, recomputed in FP64 at the end */
   double iter_residual2; /* last iterated ||r_o||^2 */
   double seconds;
+  int fallback;          /* 1: the GCR solve stalled or broke down, and plain FP64 BiCGSTAB,
+                            started from its last FP64 iterate, finished the solve */
 } qcuInvertResult;
 
 void qcuInvertParamDefault(qcuInvertParam *p);

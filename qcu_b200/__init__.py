@@ -91,6 +91,7 @@ class QcuInvertResult(ctypes.Structure):
         ("true_residual", ctypes.c_double),
         ("iter_residual2", ctypes.c_double),
         ("seconds", ctypes.c_double),
+        ("fallback", ctypes.c_int),
     ]
 
     def as_dict(self):

@@ -207,6 +207,7 @@ static void fill_result(const SolveInfo &info, qcuInvertResult *r) {
   r->true_residual = info.true_residual;
   r->iter_residual2 = info.iter_residual2;
   r->seconds = info.seconds;
+  r->fallback = info.fallback;
 }
 
 int qcuInvert(qcuGauge h, void *x, const void *b, const qcuInvertParam *p, qcuInvertResult *r) {

@@ -11,7 +11,7 @@
 
 namespace qcu {
 
-enum SolverStatus { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_BREAKDOWN = 3, ST_NAN = 4 };
+enum SolverStatus { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_BREAKDOWN = 3, ST_NAN = 4, ST_STALLED = 5 };
 
 constexpr int RED_MAXV = 40;  // largest number of doubles one reduction produces (partials stride)
 

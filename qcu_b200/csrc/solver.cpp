@@ -393,8 +393,18 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
   a.x = w.x64.data.p;
   a.r = w.r64.data.p;
   double nw[GCR_MAXK] = {};  // |W_j|^2
+  // Stagnation: a cycle (m outer steps, started from the FP64 true residual)
+  // that lowers the best true |r|^2 by less than 1 % counts as stalled;
+  // QCU_GCR_STALL_CYCLES such cycles in a row (default 3) end the GCR solve
+  // with ST_STALLED, and solve() lets plain FP64 BiCGSTAB finish from x64.
+  // (0 declares the stall after the first cycle: the host-side way the tests
+  // drive the fallback.)
+  const char *stall_env = getenv("QCU_GCR_STALL_CYCLES");
+  const int stall_limit = stall_env ? std::max(0, atoi(stall_env)) : 3;
+  double best = 0.0;
+  int stalled = 0;
   try {
-    while (info.iterations < prm.maxiter) {
+    for (int cycle = 0; info.iterations < prm.maxiter; cycle++) {
       // true residual at the start of every cycle
       d64(0, w.x64, w.tmp64, clov, 1.0);
       d64(1, w.tmp64, w.r64, clov, k2, &w.bp, 1.0, &w.x64, -1.0, RED_NORM, FIN_STORE);
@@ -407,6 +417,15 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
         info.status = ST_CONVERGED;
         break;
       }
+      if (cycle > 0) {
+        if (rr > 0.99 * best) stalled++;
+        else stalled = 0;
+        if (stalled >= stall_limit) {
+          info.status = ST_STALLED;
+          break;
+        }
+      }
+      best = cycle == 0 ? rr : std::min(best, rr);
       for (int k = 0; k < m && rr > tol2 && info.iterations < prm.maxiter; k++) {
         if (pc != 0) nn_apply_soa64(*prm.nn, dP.G, w.r64.data.p, gs.znew.data.p, st);
         if (pc == 2) {  // what the network leaves: aux = r - M_pc N(r)
@@ -550,7 +569,7 @@ SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParam
   const double kappa = prm.kappa;
   Workspace &w = workspace();
   w.prepare(kind, Vh);
-  Dsl dP{G, ctx, kind}, d64{G, ctx, SOA64};
+  Dsl dP{G, ctx, kind}, d64{G, ctx, SOA64}, dF{G, ctx, SOA64};  // dF: the FP64 fallback's operator
   if (prm.gauge_precision) {
     require(prm.gauge_precision == 16 && kind == SOA32, "solve: gauge_precision 16 is available with precision 32");
     dP.gkind = GSOA16;
@@ -577,13 +596,27 @@ SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParam
   else if (prm.x0_mode == 2) launch_uniform_soa64(Vh, w.x64.data.p, prm.x0_seed, st);
   else QCU_CUDA(cudaMemsetAsync(w.x64.data.p, 0, spinor_bytes(SOA64, Vh), st));
 
-  const VecSet vs = make_vecset(w);
+  VecSet vs = make_vecset(w);
   for (int restart = 0;; restart++) {
-    if (prm.solver == 1) {
+    if (prm.solver == 1 && !info.fallback) {
       info.status = ST_RUNNING;
       run_gcr(dP, d64, w, vs, prm, tol2, info);
+      if ((info.status == ST_STALLED || info.status == ST_BREAKDOWN || info.status == ST_NAN) &&
+          info.iterations < prm.maxiter) {
+        // the plain solver finishes: FP64 BiCGSTAB from the last FP64 iterate
+        // (from zero if that iterate is not finite), judged as always by the
+        // FP64 true residual
+        if (info.status == ST_NAN) QCU_CUDA(cudaMemsetAsync(w.x64.data.p, 0, spinor_bytes(SOA64, Vh), st));
+        info.fallback = 1;
+        w.prepare(SOA64, Vh);
+        vs = make_vecset(w);
+        info.restarts++;
+        continue;
+      }
     } else {
-      const SolverState S = run_bicgstab(dP, d64, w, vs, prm, tol2, prm.maxiter - info.iterations);
+      SolveParams pb = prm;
+      if (info.fallback) pb.delta = 0.0;  // plain: the true residual is recomputed at the end
+      const SolverState S = run_bicgstab(info.fallback ? dF : dP, d64, w, vs, pb, tol2, prm.maxiter - info.iterations);
       info.iterations += S.iter;
       info.updates += S.nupdates;
       info.status = S.status;

@@ -53,6 +53,7 @@ struct SolveInfo {
   double true_residual = 0;  // ||b - M x|| / ||b||, FP64, full two-parity system
   double iter_residual2 = 0; // last iterated ||r_pc||^2
   double seconds = 0;
+  int fallback = 0;          // GCR stalled or broke down; plain FP64 BiCGSTAB finished
 };
 
 // x, b: full two-parity spinors, PyQuda layout, complex128, device

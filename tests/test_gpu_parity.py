@@ -254,3 +254,25 @@ def test_gauge_load_waits_for_inflight_copy(q):
     finally:
         G.close()
     assert rel(host(out), O.dslash(psi, U, latt, 0, -1.0)) <= 1e-13
+
+
+def test_gcr_stall_falls_back_to_plain_fp64(q, monkeypatch):
+    """A GCR solve that stalls hands over to plain FP64 BiCGSTAB, which
+    finishes from the last FP64 iterate; the FP64 true residual decides as
+    always.  The stall is declared on the host: QCU_GCR_STALL_CYCLES=0 ends the
+    GCR solve after its first cycle."""
+    latt, kappa = [8, 8, 8, 8], 0.124
+    U, _ = _fields(latt, "smooth", 41)
+    b = O.fermion_gauss(O.full_shape(latt), 42)
+    kw = dict(tol=1e-10, maxiter=4000, solver="gcr", precision=16, inner_iters=4, inner_tol=0.5, gcr_k=2)
+    with q.Gauge(dev(U), latt, t_boundary=-1.0) as G:
+        x = empty_like_dev(O.full_shape(latt))
+        ref = G.invert(x, dev(b), kappa, **kw)
+        assert ref["status"] == 1 and ref["fallback"] == 0, ref
+        monkeypatch.setenv("QCU_GCR_STALL_CYCLES", "0")
+        x = empty_like_dev(O.full_shape(latt))
+        info = G.invert(x, dev(b), kappa, **kw)
+        assert info["status"] == 1 and info["fallback"] == 1, info
+        assert info["true_residual"] <= 1e-10
+        r = b - O.mfull(host(x), U, latt, kappa, -1.0)
+        assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05e-10
