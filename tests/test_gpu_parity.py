@@ -276,3 +276,34 @@ def test_gcr_stall_falls_back_to_plain_fp64(q, monkeypatch):
         assert info["true_residual"] <= 1e-10
         r = b - O.mfull(host(x), U, latt, kappa, -1.0)
         assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05e-10
+
+
+def test_repeated_gcr_solves_reuse_nothing_stale(q):
+    """Workspace, graphs and solver state carry nothing from one solve to the
+    next: a solve repeated after one with another kappa is bit-identical, and a
+    solve on a second gauge field of the same size (a new handle, possibly at
+    the same addresses) solves its own system."""
+    latt = [8, 8, 8, 8]
+    kw = dict(tol=1e-10, maxiter=4000, solver="gcr", precision=16, inner_iters=16, inner_tol=0.1, gcr_k=4)
+    U1, _ = _fields(latt, "smooth", 51)
+    U2, _ = _fields(latt, "smooth", 52)
+    b = O.fermion_gauss(O.full_shape(latt), 53)
+    with q.Gauge(dev(U1), latt, t_boundary=-1.0) as G:
+        xa = empty_like_dev(O.full_shape(latt))
+        ia = G.invert(xa, dev(b), 0.124, **kw)
+        xb = empty_like_dev(O.full_shape(latt))
+        ib = G.invert(xb, dev(b), 0.12, **kw)
+        xc = empty_like_dev(O.full_shape(latt))
+        ic = G.invert(xc, dev(b), 0.124, **kw)
+    assert ia["status"] == ib["status"] == ic["status"] == 1
+    assert ia["iterations"] == ic["iterations"]
+    assert np.array_equal(host(xa), host(xc))
+    for x, kappa in ((xa, 0.124), (xb, 0.12)):
+        r = b - O.mfull(host(x), U1, latt, kappa, -1.0)
+        assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05e-10
+    with q.Gauge(dev(U2), latt, t_boundary=-1.0) as G2:  # a new handle, possibly at the same addresses
+        xd = empty_like_dev(O.full_shape(latt))
+        idd = G2.invert(xd, dev(b), 0.124, **kw)
+    assert idd["status"] == 1
+    r = b - O.mfull(host(xd), U2, latt, 0.124, -1.0)
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05e-10
