@@ -12,8 +12,9 @@
 // (u, u), built once per hop, and multiplies the pair (h0, h1).  The same
 // arithmetic as the scalar hop (src/wilson_dslash.cu:56-243 of qcu), with half
 // the FP32 instructions in the projection, the product and the reconstruction.
-// The 16-bit spinors (SOA16) store the same lane pairs in one word each, so
-// one byte permute per value and one paired subtraction per pair decode them.
+// The 16-bit spinors (SOA16) store the same lane pairs in one word each: one
+// byte permute per value decodes them up to a constant offset, which the
+// projection of a hop removes itself, exactly (fmak_biased, comb_biased).
 #pragma once
 #include "fields.cuh"
 
