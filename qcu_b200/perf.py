@@ -3,6 +3,7 @@
     python -m qcu_b200.perf dslash --precision 32 --gauge-precision 16 --iters 5
     python -m qcu_b200.perf solve  --precision 32 --gauge-precision 16
     python -m qcu_b200.perf batch  --csw 1.0 --kappa 0.128
+    python -m qcu_b200.perf precisions
 
 `dslash` applies the even-odd hopping term `iters` times (after 3 warm-up
 launches) on a seeded smooth gauge field and prints the time per launch and
@@ -13,7 +14,10 @@ solves, in one batched call, the 12 point sources of a propagator on the
 main lattice together with 4 Gaussian right-hand sides on each of
 16^3 x 32, 24^3 x 48 and a second gauge field of the main lattice, and
 prints the batched wall time next to the same 24 systems solved one at a
-time.  Inputs are
+time.  `precisions` solves one system (default: the benchmark's) with plain
+FP64 BiCGSTAB, BiCGSTAB with FP64 reliable updates at 32 and 16 bits, and
+the FP64 GCR around 32- and 16-bit inner solves, and states each solution's
+difference from the FP64 one.  Inputs are
 generated on the GPU by the library's own generators; the working set of the
 default 32^3 x 64 lattice is larger than L2.
 """
@@ -41,7 +45,7 @@ def _gauge(latt, eps, seed, t_bc, csw=0.0, kappa=0.0):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["dslash", "solve", "batch"])
+    ap.add_argument("what", choices=["dslash", "solve", "batch", "precisions"])
     ap.add_argument("--latt", type=int, nargs=4, default=[32, 32, 32, 64])
     ap.add_argument("--eps", type=float, default=0.25)
     ap.add_argument("--seed", type=int, default=20251203)
@@ -79,6 +83,9 @@ def main(argv=None):
     if a.what == "batch":
         _batch(a)
         return
+    if a.what == "precisions":
+        _precisions(a)
+        return
     G, u, L = _gauge(a.latt, a.eps, a.seed, a.t_bc, a.csw, a.kappa)
     b = torch.empty(L.full, dtype=torch.complex128, device="cuda")
     q.fermion_random(b, b.numel(), 0, 7)
@@ -91,6 +98,45 @@ def main(argv=None):
     torch.cuda.synchronize()
     info["seconds"] = round(time.perf_counter() - t0, 4)
     print(json.dumps(info))
+    G.close()
+
+
+def _precisions(a):
+    """The storage precisions on one system: plain FP64 BiCGSTAB, BiCGSTAB
+    with FP64 reliable updates at 32 and 16 bits, and the FP64 GCR around
+    32- and 16-bit inner solves; per method the time of one solve after a
+    warm-up one (CUDA events on the library stream), the iterations, the FP64
+    true residual and the solution's relative difference from the FP64 one."""
+    import torch
+
+    import qcu_b200 as q
+
+    G, u, L = _gauge(a.latt, a.eps, a.seed, a.t_bc, a.csw, a.kappa)
+    del u
+    b = torch.empty(L.full, dtype=torch.complex128, device="cuda")
+    q.fermion_random(b, b.numel(), 0, 7)
+    stream = torch.cuda.ExternalStream(q.stream_handle())
+    gcr = dict(solver="gcr", inner_iters=a.inner_iters, inner_tol=a.inner_tol, gcr_k=a.gcr_k)
+    methods = [("plain FP64 BiCGSTAB", dict(precision=64, delta=0.0)),
+               ("BiCGSTAB FP32, FP64 reliable updates", dict(precision=32, delta=0.1)),
+               ("BiCGSTAB 16-bit, FP64 reliable updates", dict(precision=16, delta=0.1)),
+               ("FP64 GCR, inner FP32 / 16-bit links", dict(precision=32, gauge_precision=16, **gcr)),
+               ("FP64 GCR, inner 16-bit", dict(precision=16, **gcr))]
+    x64 = None
+    for name, kw in methods:
+        x = torch.empty_like(b)
+        G.invert(x, b, a.kappa, tol=a.tol, maxiter=20000, clover=a.csw != 0.0, **kw)  # warm-up
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        info = G.invert(x, b, a.kappa, tol=a.tol, maxiter=20000, clover=a.csw != 0.0, **kw)
+        e1.record(stream)
+        e1.synchronize()
+        if x64 is None:
+            x64 = x.clone()
+        diff = float(torch.linalg.vector_norm(x - x64) / torch.linalg.vector_norm(x64))
+        print(json.dumps({"method": name, "seconds": round(e0.elapsed_time(e1) / 1e3, 4),
+                          "iterations": info["iterations"], "status": info["status"],
+                          "true_residual": info["true_residual"], "rel_diff_vs_fp64": diff}))
     G.close()
 
 
