@@ -307,15 +307,17 @@ class Gauge:
         return ms.value
 
 
-def invert_batch(systems, tol: float = 1e-10, maxiter: int = 10000, precision: int = 32, gauge_precision: int = 16,
+def invert_batch(systems, tol: float = 1e-10, maxiter: int = 10000, precision: int = 16, gauge_precision: int = 0,
                  inner_iters: int = 96, inner_tol: float = 0.05, gcr_k: int = 4):
     """Solve every right-hand side of every system together (qcuInvertBatch).
 
     systems: sequence of (gauge, x, b, kappa, clover) with `gauge` a Gauge and
     x, b contiguous complex128 CUDA tensors of nrhs full spinors
     ([nrhs, 2, Lt, Lz, Ly, Lx/2, 4, 3]).  Lattices may differ between
-    systems.  Returns (one result dict per right-hand side in system order,
-    the tunables the autotuner chose)."""
+    systems.  The inner solve runs on 16-bit spinors and links by default
+    (precision=32 with gauge_precision=16 or 0, or 64, for the others).
+    Returns (one result dict per right-hand side in system order, the
+    tunables the autotuner chose)."""
     sys_arr = (QcuBatchSystem * len(systems))()
     nrhs_total = 0
     for i, (G, x, b, kappa, clover) in enumerate(systems):
