@@ -269,7 +269,7 @@ static cudaGraphExec_t capture_inner_solve(Dsl &dP, Workspace &w, const VecSet &
 // convergence and no host involvement.  `iters_out` is not known at capture
 // time: the caller reads st->iter after each replay.
 static cudaGraphExec_t capture_inner_solve_while(Dsl &dP, Workspace &w, const VecSet &vs, double kappa, bool clov,
-                                                 int iters, Spinor &z_out) {
+                                                 int iters, Spinor &z_out, long long &per_iter) {
   Context &ctx = dP.ctx;
   const int Vh = dP.G.g.Vh, kind = dP.kind;
   const double k2 = kappa * kappa;
@@ -298,6 +298,7 @@ static cudaGraphExec_t capture_inner_solve_while(Dsl &dP, Workspace &w, const Ve
     QCU_CUDA(cudaGraphAddNode(&loop, g, &init_node, 1, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     QCU_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, mode));
+    const long long body0 = launch_count();
     launch_pupdate(kind, Vh, vs, ctx.st, GATE_NOT_DONE, st);
     dP(0, w.p, w.tmp, clov, 1.0, nullptr, 0, nullptr, 0, RED_NONE, FIN_STORE, nullptr, GATE_NOT_DONE);
     dP(1, w.tmp, w.v, clov, -k2, &w.p, 1.0, nullptr, 0, RED_DOT_RT, FIN_ALPHA, &w.rt, GATE_NOT_DONE);
@@ -306,6 +307,7 @@ static cudaGraphExec_t capture_inner_solve_while(Dsl &dP, Workspace &w, const Ve
     dP(1, w.tmp, w.t, clov, -k2, &w.s, 1.0, nullptr, 0, RED_TS_TT, FIN_OMEGA, nullptr, GATE_NOT_DONE);
     launch_xrupdate(kind, Vh, vs, ctx, GATE_NOT_DONE, st);
     launch_loop_cond(ctx.st, h, (unsigned)iters + 2u, st);
+    per_iter = launch_count() - body0;  // kernels per pass of the loop body
     QCU_CUDA(cudaStreamEndCapture(st, &body));
     QCU_CUDA(cudaStreamBeginCaptureToGraph(st, g, &loop, nullptr, 1, mode));
     launch_convert(w.x.kind, SOA64, Vh, w.x.data.p, w.x.norm.as<float>(), z_out.data.p, nullptr, st);
@@ -374,10 +376,11 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
   VecSet vin = vs;
   vin.r64 = pc == 2 ? w.aux.data.p : w.r64.data.p;
   long long nodes = 0;  // 0: device-side WHILE loop (launches counted from the iteration count)
+  long long per_iter = 8;  // kernels per pass of the WHILE body (measured at capture)
   cudaGraphExec_t inner = nullptr;
   if (pc != 1) {
     try {
-      inner = capture_inner_solve_while(dP, w, vin, kappa, clov, prm.inner_iters, gs.zin);
+      inner = capture_inner_solve_while(dP, w, vin, kappa, clov, prm.inner_iters, gs.zin, per_iter);
     } catch (const Error &) {
       // conditional graph nodes unavailable: fixed-length capture with gated iterations
       inner = capture_inner_solve(dP, w, vin, kappa, clov, prm.inner_iters, gs.zin, nodes);
@@ -451,11 +454,11 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
             a.beta[2 * j + 1] = S.sums[2 * j + 1] / nw[j];
           }
           info.iterations += pc == 1 ? 1 : S.iter;  // inner iterations of this step
-          if (pc != 1 && !nodes) note_launch(2 + 8LL * std::max(S.iter, 1));
+          if (pc != 1 && !nodes) note_launch(2 + per_iter * std::max(S.iter, 1));
         } else {
           const int it = pc == 1 ? 1 : read_state(ctx).iter;
           info.iterations += it;
-          if (pc != 1 && !nodes) note_launch(2 + 8LL * std::max(it, 1));
+          if (pc != 1 && !nodes) note_launch(2 + per_iter * std::max(it, 1));
         }
         launch_gcr_orth(Vh, a, ctx, st);
         SolverState S = read_state(ctx);
