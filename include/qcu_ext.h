@@ -139,8 +139,13 @@ int qcuFermionRandom(void *psi, long long n_complex, int kind, unsigned long lon
  * on success, non-zero with qcuGetLastError() set otherwise.
  *  - at most qcuNoAllocMaxSites() = 32768 sites per parity (a 16^4 lattice);
  *    larger lattices are rejected with an error;
- *  - the first call on a device sets up the scratch address with that device
- *    current; make it before any stream capture;
+ *  - the driver reserves the array on a device when the library's device code
+ *    is first used there (lazy module loading, the CUDA 12 default; at load
+ *    time under CUDA_MODULE_LOADING=EAGER): under a hard memory cap, make the
+ *    first call early;
+ *  - every call synchronises the device and runs on the legacy default
+ *    stream: make no call while a stream of the process is being captured;
+ *    a call cannot be captured;
  *  - all calls share the scratch: calls that overlap on the GPU race. */
 int dslashCloverQcuNoAlloc(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, int parity);
 int qcuNoAllocMaxSites(void);

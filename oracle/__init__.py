@@ -22,6 +22,17 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+
+def reference_root() -> str:
+    """Root of qcu's source tree, read only by the recipes that rebuild qcu
+    and PyQuda's binding and by the scripts that make fixtures: the
+    ``QCU_REFERENCE`` environment variable, else ``reference/`` beside this
+    repository's own directory.  Nothing that runs on a GPU needs it."""
+    env = os.environ.get("QCU_REFERENCE")
+    if env:
+        return os.path.abspath(env)
+    return os.path.normpath(os.path.join(_HERE, "..", "..", "reference"))
 _lib = None
 
 _c128p = ctypes.c_void_p

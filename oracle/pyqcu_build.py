@@ -10,7 +10,7 @@ Reads the reference tree (read-only), writes only under oracle/_ref/:
     oracle/_ref/pyquda/{__init__.py, pointer*.so, pyqcu*.so}
 The pyqcu module links libqcu.so with an rpath to qcu_b200/ of this checkout.
 
-    python oracle/pyqcu_build.py [--ref /root/reference]
+    python oracle/pyqcu_build.py [--ref <qcu source tree>]   (default: $QCU_REFERENCE, else ../reference)
 """
 import argparse
 import os
@@ -62,7 +62,10 @@ def build(ref: str) -> str:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    sys.path.insert(0, REPO)
+    from oracle import reference_root
+
+    ap.add_argument("--ref", default=reference_root())
     a = ap.parse_args()
     print(build(a.ref))
 

@@ -3,8 +3,9 @@
 # oracle/_ref/.  Uses oracle/ref_stub/mpi.h in place of an MPI install; links
 # the system NCCL, cuBLAS and cuRAND that qcu needs (CMakeLists.txt:19-23).
 # The product never loads the result.
-REF     ?= /root/reference
 HERE    := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
+# qcu's source tree: $(QCU_REFERENCE), else reference/ beside this repository
+REF     ?= $(if $(QCU_REFERENCE),$(QCU_REFERENCE),$(abspath $(HERE)../../reference))
 OUT     := $(HERE)_ref
 NVCC    ?= nvcc
 SRCS    := draft wilson_dslash clover_dslash lattice_cuda bistabcg \

@@ -43,10 +43,7 @@ struct BatchCache {
     memset(coef_host, 0, sizeof(BatchCoef) * BATCH_MAX_RHS);
   }
 };
-BatchCache &cache() {
-  static BatchCache *c = new BatchCache();  // intentionally never destroyed (lives until exit)
-  return *c;
-}
+BatchCache &cache() { return per_device<BatchCache>(context()); }
 
 // Tile table over "units" (a rhs, or a group of rhs sharing a lattice):
 // every unit's sites in blocks of `sites`; tiles sorted by the position of

@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <map>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -102,10 +103,28 @@ struct Context {
   double *partials = nullptr;      // blocks * RED_MAXV doubles (grown to the largest grid used)
   size_t partials_blocks = 0;
   int sms = 148;                   // multiprocessors of the device
+  // scratch of the legacy clover call (dslashCloverQcu): the inverse clover
+  // of the output parity and its zero-pivot counter.  Per device, used only
+  // under `mu`; allocated on first use and kept until exit.
+  DevBuf *legacy_clover = nullptr;
+  DevBuf *legacy_bad = nullptr;
   std::mutex mu;
   void ensure_partials(size_t blocks);
 };
 Context &context();  // current device's context
+
+// One T per device, created on first use and kept until exit: the work
+// buffers of a solve live on the device they were allocated on, so each
+// device gets its own (callers hold that device's Context::mu while using it).
+template <typename T>
+T &per_device(const Context &ctx) {
+  static std::mutex mu;
+  static std::map<int, T *> objs;
+  std::lock_guard<std::mutex> lk(mu);
+  T *&p = objs[ctx.device];
+  if (p == nullptr) p = new T();
+  return *p;
+}
 
 // ---------------------------------------------------------------- kernels (launchers)
 struct DslashArgs {

@@ -43,11 +43,8 @@ struct NNet {
   }
 };
 
-// staging spinor for the complex128 <-> complex64 conversions (never freed)
-static Spinor &stage() {
-  static Spinor *t = new Spinor();
-  return *t;
-}
+// staging spinor for the complex128 <-> complex64 conversions (one per device, never freed)
+static Spinor &stage() { return per_device<Spinor>(context()); }
 
 static void refresh_bf16(NNet &n, cudaStream_t s) { launch_to_bf16(NN_NPARAM, n.w.as<float>(), n.w16.as<uint32_t>(), s); }
 

@@ -11,51 +11,47 @@
 //
 // Limits and rules:
 //  * at most NOALLOC_MAX_VH sites per parity (16^4 = 32768, e.g. 16^4, 16^3x8,
-//    8^3x64); the array is 32768 * 576 B = 18 MiB and every GPU that loads
-//    the library holds it until the process exits;
-//  * the first call on a device does a one-time set-up with that device
-//    current: it looks up the array's device address (and the driver may
-//    reserve the kernels' local memory at their first launch); make that first
-//    call before any stream capture;
+//    8^3x64); the array is 32768 * 576 B = 18 MiB per device;
+//  * the driver reserves that array on a device when the library's device
+//    code is loaded there: with lazy module loading (the CUDA 12 default)
+//    that is the first use on that device, typically this entry point's first
+//    call; with CUDA_MODULE_LOADING=EAGER it is when the library is loaded.
+//    A caller under a hard memory cap should make the first call early, while
+//    the 18 MiB are still available; the array is then held until the process
+//    exits;
+//  * every call looks up the array's device address with that device current
+//    (cudaGetSymbolAddress, cheap once the module is loaded), so a call after
+//    cudaDeviceReset finds the array of the new context;
+//  * every call synchronises the device and runs on the legacy default
+//    stream: no call may be made while any stream of the process is being
+//    captured, and a call cannot itself be captured;
 //  * every call reuses the same array, which keeps the previous call's
-//    contents; calls that overlap on the GPU (from several host threads, or
-//    on different streams) race on it.  The call itself runs on the legacy
-//    default stream and returns after its work has completed.
-#include <mutex>
-
+//    contents; calls that overlap on the GPU (from several host threads)
+//    race on it.  A call returns after its work has completed.
 #include "internal.h"
 
 namespace qcu {
 
 constexpr int NOALLOC_MAX_VH = 32768;
-constexpr int NOALLOC_MAX_DEVICES = 64;
 
 // scratch: packed inverse clover (2 chiral blocks x 18 double2 per site) and
 // the zero-pivot counter
 static __device__ __align__(256) double2 g_noalloc_clover[(size_t)NOALLOC_MAX_VH * 2 * 18];
-static __device__ __align__(256) int g_noalloc_bad[64];
+static __device__ __align__(256) int g_noalloc_bad;
 
 struct NoAllocSlot {
   void *clover = nullptr;
   int *bad = nullptr;
 };
 
-// device address of the scratch on the current device (looked up once per device)
+// device addresses of the scratch in the current device's context
 static NoAllocSlot noalloc_slot() {
-  static std::mutex mu;
-  static NoAllocSlot slots[NOALLOC_MAX_DEVICES];
-  int dev = 0;
-  QCU_CUDA(cudaGetDevice(&dev));
-  require(dev >= 0 && dev < NOALLOC_MAX_DEVICES, "device ordinal out of range");
-  std::lock_guard<std::mutex> lk(mu);
-  NoAllocSlot &s = slots[dev];
-  if (s.clover == nullptr) {
-    void *c = nullptr, *b = nullptr;
-    QCU_CUDA(cudaGetSymbolAddress(&c, g_noalloc_clover));
-    QCU_CUDA(cudaGetSymbolAddress(&b, g_noalloc_bad));
-    s.clover = c;
-    s.bad = static_cast<int *>(b);
-  }
+  NoAllocSlot s;
+  void *c = nullptr, *b = nullptr;
+  QCU_CUDA(cudaGetSymbolAddress(&c, g_noalloc_clover));
+  QCU_CUDA(cudaGetSymbolAddress(&b, g_noalloc_bad));
+  s.clover = c;
+  s.bad = static_cast<int *>(b);
   return s;
 }
 

@@ -83,10 +83,7 @@ struct Workspace {
     x.alloc(kind == SOA64 ? SOA64 : SOA32, Vh);
   }
 };
-Workspace &workspace() {
-  static Workspace *w = new Workspace();  // intentionally never destroyed (lives until exit)
-  return *w;
-}
+Workspace &workspace() { return per_device<Workspace>(context()); }
 }  // namespace
 
 void Dsl::operator()(int par, const Spinor &in, Spinor &out, bool clover, double a, const Spinor *x1, double b1,
@@ -342,10 +339,7 @@ struct GcrSpace {
     zin.alloc(SOA64, Vh);
   }
 };
-GcrSpace &gcr_space() {
-  static GcrSpace *g = new GcrSpace();  // intentionally never destroyed
-  return *g;
-}
+GcrSpace &gcr_space() { return per_device<GcrSpace>(context()); }
 }  // namespace
 
 // Flexible GCR(m) on M_pc in FP64 with the inner solve above as right
@@ -734,7 +728,11 @@ void legacy_dslash(void *out, const void *in, const void *gauge, const int latt[
   d.parity = parity;
   d.t_bc = 1.0;
   d.a = 1.0;
-  static DevBuf *cl = new DevBuf(), *bad = new DevBuf();  // reused across calls, never freed
+  if (clover && ctx.legacy_clover == nullptr) {  // this device's scratch, reused across calls, never freed
+    ctx.legacy_clover = new DevBuf();
+    ctx.legacy_bad = new DevBuf();
+  }
+  DevBuf *cl = ctx.legacy_clover, *bad = ctx.legacy_bad;
   if (clover) {
     // qcu builds the clover of the output parity with unit normalisation on
     // every call (src/nccl_clover_dslash.cu:27-61)

@@ -307,3 +307,44 @@ def test_repeated_gcr_solves_reuse_nothing_stale(q):
     assert idd["status"] == 1
     r = b - O.mfull(host(xd), U2, latt, 0.124, -1.0)
     assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.05e-10
+
+
+def test_dslashCloverQcu_threads_share_one_device(q):
+    """dslashCloverQcu keeps its clover scratch in the calling device's
+    context, under that context's lock: calls from two host threads on one
+    device give, call after call, exactly the results of serial calls."""
+    import threading
+
+    cases = [([8, 8, 8, 8], 41, 0), ([4, 4, 8, 8], 42, 1)]
+    inputs, refs = [], []
+    for latt, seed, par in cases:
+        U, psi = _fields(latt, "smooth", seed)
+        dU, dpsi = dev(U), dev(psi[1 - par])
+        out = empty_like_dev(O.half_shape(latt))
+        q.dslashCloverQcu(out, dpsi, dU, q.QcuParam(latt), par)
+        assert q.last_error()[0] == 0
+        A = O.clover_build(U, latt, par, 1.0)
+        ref = O.clover_apply(O.clover_invert(A), O.dslash(psi[1 - par], U, latt, par, 1.0))
+        assert rel(host(out), ref) <= 1e-11  # smooth links: the inverse is well conditioned
+        inputs.append((latt, dU, dpsi, par))
+        refs.append(host(out))
+    errors = []
+
+    def worker(k):
+        import torch
+
+        torch.cuda.set_device(0)
+        latt, dU, dpsi, par = inputs[k]
+        for _ in range(6):
+            out = empty_like_dev(O.half_shape(latt))
+            q.dslashCloverQcu(out, dpsi, dU, q.QcuParam(latt), par)
+            code, msg = q.last_error()
+            if code != 0 or not np.array_equal(host(out), refs[k]):
+                errors.append((k, code, msg))
+
+    th = [threading.Thread(target=worker, args=(k,)) for k in range(len(cases))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errors, errors

@@ -93,5 +93,7 @@ def test_bistabcg_through_pyqcu(pyqcu):
                         ptr.ndarrayDataPointer(dU.reshape(-1), True), _param(mod, latt), _param(mod, [1, 1, 1, 1]))
     xs = host(x)
     r = b - O.mfull(xs, U, latt, 0.125, 1.0)
-    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-3
-    assert np.linalg.norm(r[1]) ** 2 < 1e-6  # the odd residual is what qcu's criterion bounds (absolute)
+    # qcu's criterion: ||r_o||^2 < 1e-9, absolute (include/define.h:68, lattice_bistabcg.h:301); x_e is
+    # rebuilt exactly from x_o, so the even residual vanishes and the full residual obeys the same bound
+    assert np.linalg.norm(r) ** 2 < 1e-9
+    assert np.linalg.norm(r[0]) ** 2 < 1e-20

@@ -6,7 +6,9 @@ import pytest
 
 import oracle as O
 
-WEAK = "/root/reference/python/PyQuda/tests/weak_field.lime"
+# PyQuda's own test configuration (python/PyQuda/tests/weak_field.lime), copied
+# beside the other fixtures by tests/golden/make_golden.py
+WEAK = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "weak_field.lime")
 
 
 def _su3_error(U):

@@ -24,6 +24,27 @@ def _inputs(latt, kind, seed):
     return dev(U), dev(psi), U, psi
 
 
+def _only_process_on_device():
+    """True when NVML lists no compute process on the current GPU besides this one."""
+    import os
+
+    import torch
+
+    try:
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            procs = pynvml.nvmlDeviceGetComputeRunningProcesses(h)
+            return all(p.pid == os.getpid() for p in procs)
+        finally:
+            pynvml.nvmlShutdown()
+    except Exception:
+        return False
+
+
 def test_no_alloc_matches_dslashCloverQcu_on_two_calls_in_a_row():
     import qcu_b200 as q
 
@@ -50,12 +71,19 @@ def test_no_alloc_allocates_nothing_and_rejects_oversize():
     latt, kind, seed, parity = CASES[0]
     dU, dpsi, _, _ = _inputs(latt, kind, seed)
     out = empty_like_dev(O.half_shape(latt))
-    assert q.dslashCloverQcuNoAlloc(out, dpsi, dU, q.QcuParam(latt), parity) == 0  # set-up done
+    assert q.dslashCloverQcuNoAlloc(out, dpsi, dU, q.QcuParam(latt), parity) == 0  # module loaded
     torch.cuda.synchronize()
+    reserved_before = torch.cuda.memory_reserved()
     free_before = torch.cuda.mem_get_info()[0]
     assert q.dslashCloverQcuNoAlloc(out, dpsi, dU, q.QcuParam(latt), 1 - parity) == 0
     torch.cuda.synchronize()
-    assert torch.cuda.mem_get_info()[0] == free_before
+    free_after = torch.cuda.mem_get_info()[0]
+    assert torch.cuda.memory_reserved() == reserved_before  # nothing through torch's allocator
+    # The free-memory figure is device-wide: another process on the GPU would
+    # move it.  Exact equality is asserted only when this process is the only
+    # one the driver lists on the device.
+    if _only_process_on_device():
+        assert free_after == free_before
     # beyond the static scratch: a clear error, nothing written
     big = [32, 32, 32, 32]
     assert O.vh(big) > q.noalloc_max_sites()
