@@ -123,6 +123,22 @@ typedef struct {
 int qcuInvertBatch(const qcuBatchSystem *systems, int n_systems, const qcuInvertParam *p, qcuInvertResult *results,
                    qcuBatchTune *tune);
 
+/* Operator check of the batched solver's inner kernels (no counterpart in
+ * qcu, whose solver takes one right-hand side).  For every right-hand side j
+ * of every system, the odd half b_o of b_j is stored in the inner precision
+ * (precision / gauge_precision as for qcuInvertBatch), and the batched
+ * hopping kernels of the inner solve, launched with the tunables `tune`
+ * (sites per block, right-hand sides per thread, tensor-core mode 0/1/2),
+ * compute, written to x_j as complex128:
+ *   even half  [A_e^-1] D_eo b_o                       (first half of M_pc)
+ *   odd half   M_pc b_o = b_o - kappa^2 [A_o^-1] D_oe [A_e^-1] D_eo b_o
+ * with both fused reductions of the inner iteration:
+ *   dots[5i+0..1] = <b_o, M_pc b_o>, dots[5i+2..3] = <M_pc b_o, b_o>,
+ *   dots[5i+4] = |M_pc b_o|^2                          (rhs i in system order).
+ * Clover is applied for systems with use_clover. */
+int qcuBatchApplyMatPC(const qcuBatchSystem *systems, int n_systems, int precision, int gauge_precision,
+                       const qcuBatchTune *tune, double *dots);
+
 /* seeded generators, PyQuda layout complex128 on the device.
  * gauge kind: 0 Haar SU(3), 1 exp(i eps H) reunitarised, 2 unit links.
  * fermion kind: 0 complex normal N(0,1) per component, 1 uniform (0,1]. */

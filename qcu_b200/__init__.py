@@ -139,6 +139,8 @@ _lib.qcuInvertParamDefault.restype = None
 _lib.qcuInvert.argtypes = [_vp, _vp, _vp, ctypes.POINTER(QcuInvertParam), ctypes.POINTER(QcuInvertResult)]
 _lib.qcuInvertBatch.argtypes = [ctypes.POINTER(QcuBatchSystem), ctypes.c_int, ctypes.POINTER(QcuInvertParam),
                                 ctypes.POINTER(QcuInvertResult), ctypes.POINTER(QcuBatchTune)]
+_lib.qcuBatchApplyMatPC.argtypes = [ctypes.POINTER(QcuBatchSystem), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(QcuBatchTune), ctypes.c_void_p]
 _lib.qcuGaugeRandom.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong]
 _lib.qcuFermionRandom.argtypes = [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_ulonglong]
 _lib.qcuGetStream.restype = _vp
@@ -318,6 +320,18 @@ def invert_batch(systems, tol: float = 1e-10, maxiter: int = 10000, precision: i
     (precision=32 with gauge_precision=16 or 0, or 64, for the others).
     Returns (one result dict per right-hand side in system order, the
     tunables the autotuner chose)."""
+    sys_arr, nrhs_total = _batch_systems(systems)
+    p = QcuInvertParam()
+    _lib.qcuInvertParamDefault(ctypes.byref(p))
+    p.tol, p.maxiter, p.precision, p.gauge_precision = tol, maxiter, precision, gauge_precision
+    p.solver, p.inner_iters, p.inner_tol, p.gcr_k = 1, inner_iters, inner_tol, gcr_k
+    res = (QcuInvertResult * max(nrhs_total, 1))()
+    tune = QcuBatchTune()
+    _check(_lib.qcuInvertBatch(sys_arr, len(systems), ctypes.byref(p), res, ctypes.byref(tune)))
+    return [res[i].as_dict() for i in range(nrhs_total)], tune.as_dict()
+
+
+def _batch_systems(systems):
     sys_arr = (QcuBatchSystem * len(systems))()
     nrhs_total = 0
     for i, (G, x, b, kappa, clover) in enumerate(systems):
@@ -332,14 +346,28 @@ def invert_batch(systems, tol: float = 1e-10, maxiter: int = 10000, precision: i
         sys_arr[i].x = _ptr(x)
         sys_arr[i].b = _ptr(b)
         nrhs_total += n
-    p = QcuInvertParam()
-    _lib.qcuInvertParamDefault(ctypes.byref(p))
-    p.tol, p.maxiter, p.precision, p.gauge_precision = tol, maxiter, precision, gauge_precision
-    p.solver, p.inner_iters, p.inner_tol, p.gcr_k = 1, inner_iters, inner_tol, gcr_k
-    res = (QcuInvertResult * max(nrhs_total, 1))()
+    return sys_arr, nrhs_total
+
+
+def batch_apply_matpc(systems, precision: int = 16, gauge_precision: int = 0, dslash_threads: int = 128,
+                      dslash_rhs: int = 1, mma: int = 0, blas_sites: int = 256):
+    """The batched solver's inner operator, applied once (qcuBatchApplyMatPC).
+
+    systems as for invert_batch.  For every right-hand side j, the kernels of
+    the batched inner solve, with the given tunables, write to x[j]: the even
+    half [A_e^-1] D_eo b_o and the odd half M_pc b_o, both computed from b[j]'s
+    odd half stored in the inner precision.  Returns an [nrhs, 5] numpy array
+    of the fused reductions: Re/Im <b_o, M_pc b_o>, Re/Im <M_pc b_o, b_o>,
+    |M_pc b_o|^2."""
+    import numpy as np
+
+    sys_arr, nrhs = _batch_systems(systems)
     tune = QcuBatchTune()
-    _check(_lib.qcuInvertBatch(sys_arr, len(systems), ctypes.byref(p), res, ctypes.byref(tune)))
-    return [res[i].as_dict() for i in range(nrhs_total)], tune.as_dict()
+    tune.dslash_threads, tune.dslash_rhs, tune.blas_sites, tune.mma = dslash_threads, dslash_rhs, blas_sites, mma
+    dots = np.zeros((max(nrhs, 1), 5))
+    _check(_lib.qcuBatchApplyMatPC(sys_arr, len(systems), int(precision), int(gauge_precision), ctypes.byref(tune),
+                                   dots.ctypes.data))
+    return dots[:nrhs]
 
 
 def point_sources(latt, origin, device="cuda"):

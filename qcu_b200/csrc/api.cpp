@@ -245,6 +245,33 @@ int qcuInvertBatch(const qcuBatchSystem *systems, int n_systems, const qcuInvert
   QCU_API_END
 }
 
+int qcuBatchApplyMatPC(const qcuBatchSystem *systems, int n_systems, int precision, int gauge_precision,
+                       const qcuBatchTune *tune, double *dots) {
+  QCU_API_BEGIN
+  require(systems != nullptr && tune != nullptr && dots != nullptr && n_systems > 0,
+          "null systems/tune/dots pointer or no systems");
+  std::vector<BatchSystem> sys(n_systems);
+  for (int i = 0; i < n_systems; i++) {
+    require(systems[i].gauge != nullptr, "batch: null gauge handle");
+    sys[i].G = systems[i].gauge->h;
+    sys[i].nrhs = systems[i].nrhs;
+    sys[i].kappa = systems[i].kappa;
+    sys[i].use_clover = systems[i].use_clover;
+    sys[i].x = systems[i].x;
+    sys[i].b = systems[i].b;
+  }
+  SolveParams p;
+  p.precision = precision;
+  p.gauge_precision = gauge_precision;
+  BatchTune t;
+  t.dslash_threads = tune->dslash_threads;
+  t.dslash_rhs = tune->dslash_rhs;
+  t.blas_sites = tune->blas_sites;
+  t.mma = tune->mma;
+  solve_batch(sys, p, nullptr, &t, dots);
+  QCU_API_END
+}
+
 int qcuGaugeRandom(void *gauge, const int latt[4], int kind, double eps, unsigned long long seed) {
   QCU_API_BEGIN
   require(gauge != nullptr, "gauge pointer is null");

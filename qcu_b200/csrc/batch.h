@@ -127,6 +127,10 @@ struct BatchSystem {
 // 64) over all rhs of all systems,
 // captured once as a CUDA graph with a device-side WHILE loop.  One SolveInfo
 // per rhs, in system order.
-std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const SolveParams &prm, BatchTune *tune_out);
+// force_tune: use these tunables (no autotuning).  apply_dots: instead of
+// solving, apply the batched inner operator once per rhs (apply mode, below)
+// and write 5 doubles per rhs there.
+std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const SolveParams &prm, BatchTune *tune_out,
+                                   const BatchTune *force_tune = nullptr, double *apply_dots = nullptr);
 
 }  // namespace qcu

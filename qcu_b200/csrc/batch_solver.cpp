@@ -72,7 +72,8 @@ std::vector<int2> make_tiles(const std::vector<int> &unit_vh, int sites) {
 
 }  // namespace
 
-std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const SolveParams &prm, BatchTune *tune_out) {
+std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const SolveParams &prm, BatchTune *tune_out,
+                                   const BatchTune *force_tune, double *apply_dots) {
   const auto t0 = std::chrono::steady_clock::now();
   require(!sys.empty(), "batch: no systems");
   require(prm.maxiter > 0 && prm.inner_iters > 0 && prm.gcr_k > 0, "batch: maxiter, inner_iters, gcr_k must be > 0");
@@ -190,6 +191,13 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
     require(f.blas_sites >= 128 && f.blas_sites % 128 == 0, "QCU_BATCH_TUNE: blas_sites must be a multiple of 128");
     require(f.dslash_rhs >= 1 && f.dslash_rhs <= BATCH_MAX_NR, "QCU_BATCH_TUNE: rhs per group out of range");
     tune = f;
+    need_tune = false;
+  }
+  if (force_tune) {
+    require(force_tune->blas_sites >= 128 && force_tune->blas_sites % 128 == 0,
+            "batch: blas_sites must be a multiple of 128");
+    require(force_tune->dslash_rhs >= 1 && force_tune->dslash_rhs <= BATCH_MAX_NR, "batch: rhs per group out of range");
+    tune = *force_tune;
     need_tune = false;
   }
   const bool tune_log = getenv("QCU_TUNE_LOG") != nullptr;
@@ -358,6 +366,46 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
     set_launch_count(launches0);  // tuning launches are not part of the solve
   }
   if (tune_out) *tune_out = tune;
+
+  // ---- apply mode: the inner operator of the batched solve, once, as an
+  //      operator (the kernels and launch shapes the inner iteration uses)
+  if (apply_dots) {
+    for (int r = 0; r < R; r++) {
+      const size_t half = spinor_bytes(AOS64, Vh[r]);
+      const void *bo = static_cast<const char *>(rl[r].s->b) + 2 * half * rl[r].j + half;
+      RhsBufs &B = *c.rhs[r];
+      for (int k : {BV_P, BV_RT})
+        launch_convert(AOS64, kind, Vh[r], bo, nullptr, B.v[k].data.p, B.v[k].norm.as<float>(), st);
+    }
+    // tmp = [A_e^-1] D_eo p;  v = p - kappa^2 [A_o^-1] D_oe tmp  with <rt, v> (rt = p),
+    // then the same with the other fused reduction: t = M_pc p with <t, p>, |t|^2
+    BDslOp d0;
+    d0.in = BV_P, d0.out = BV_TMP, d0.parity = 0, d0.clover = clov_any, d0.gate = BG_ALWAYS;
+    BDslOp d1 = d0;
+    d1.in = BV_TMP, d1.out = BV_V, d1.parity = 1, d1.a0 = 0, d1.ak2 = -1, d1.x1 = BV_P, d1.b1 = 1,
+    d1.red = RED_DOT_RT, d1.fin = FIN_STORE, d1.rt = BV_RT;
+    inner_dsl(d0);
+    inner_dsl(d1);
+    SolverState *S = read_states();
+    for (int r = 0; r < R; r++) apply_dots[5 * r] = S[r].sums[0], apply_dots[5 * r + 1] = S[r].sums[1];
+    BDslOp d2 = d1;
+    d2.out = BV_T, d2.red = RED_TS_TT, d2.rt = -1;
+    inner_dsl(d0);
+    inner_dsl(d2);
+    S = read_states();
+    for (int r = 0; r < R; r++)
+      for (int k = 0; k < 3; k++) apply_dots[5 * r + 2 + k] = S[r].sums[k];
+    for (int r = 0; r < R; r++) {
+      const size_t half = spinor_bytes(AOS64, Vh[r]);
+      char *x = static_cast<char *>(rl[r].s->x) + 2 * half * rl[r].j;
+      RhsBufs &B = *c.rhs[r];
+      launch_convert(kind, AOS64, Vh[r], B.v[BV_TMP].data.p, B.v[BV_TMP].norm.as<float>(), x, nullptr, st);
+      launch_convert(kind, AOS64, Vh[r], B.v[BV_V].data.p, B.v[BV_V].norm.as<float>(), x + half, nullptr, st);
+      info[r].status = ST_CONVERGED;
+    }
+    QCU_CUDA(cudaStreamSynchronize(st));
+    return info;
+  }
 
   // ---- inner solve graph: init, WHILE(batched BiCGSTAB iteration), z = x
   cudaGraph_t g = nullptr;

@@ -348,3 +348,39 @@ def test_dslashCloverQcu_threads_share_one_device(q):
     for t in th:
         t.join()
     assert not errors, errors
+
+
+def test_dslashQcu_on_pyquda_weak_field_lime(q):
+    """A gauge file this project did not write: PyQuda's own test
+    configuration (python/PyQuda/tests/weak_field.lime, 4^3 x 8), read by
+    qcu_b200.ildg, through dslashQcu, dslashCloverQcu and a solve, against
+    the oracle."""
+    import os
+
+    from qcu_b200 import ildg
+
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "weak_field.lime")
+    U, latt, info = ildg.read_ildg(path)
+    assert latt == [4, 4, 4, 8] and info["checksum"] == "ok"
+    psi = O.fermion_gauss(O.full_shape(latt), 77)
+    dU, dpsi = dev(U), dev(psi)
+    for p in (0, 1):
+        out = empty_like_dev(O.half_shape(latt))
+        q.dslashQcu(out, dpsi[1 - p], dU, q.QcuParam(latt), p)
+        assert q.last_error()[0] == 0
+        assert rel(host(out), O.dslash(psi[1 - p], U, latt, p)) <= 1e-13
+        out = empty_like_dev(O.half_shape(latt))
+        q.dslashCloverQcu(out, dpsi[1 - p], dU, q.QcuParam(latt), p)
+        assert q.last_error()[0] == 0
+        A = O.clover_build(U, latt, p, 1.0)
+        ref = O.clover_apply(O.clover_invert(A), O.dslash(psi[1 - p], U, latt, p))
+        assert rel(host(out), ref) <= 1e-12
+    # a clover solve on the file's field (antiperiodic t, csw = 1), checked with the oracle's operator
+    kappa = 0.12
+    A = [O.clover_build(U, latt, p, kappa) for p in (0, 1)]
+    x = empty_like_dev(O.full_shape(latt))
+    with q.Gauge(dU, latt, t_boundary=-1.0, clover_coeff=kappa) as G:
+        res = G.invert(x, dpsi, kappa, tol=1e-10, precision=16, solver="gcr", clover=True)
+    assert res["status"] == 1
+    r = psi - O.mfull(host(x), U, latt, kappa, -1.0, True, A[0], A[1])
+    assert np.linalg.norm(r) / np.linalg.norm(psi) <= 1.05e-10
