@@ -1,21 +1,32 @@
 #!/usr/bin/env python
-"""Benchmark of qcu's hot path on B200: even-odd preconditioned BiCGSTAB for
-the Wilson operator on a 32^3 x 64 lattice.
+"""Benchmark of qcu's hot path on B200: even-odd preconditioned solves of the
+Wilson (and clover) operator on a 32^3 x 64 lattice.
 
 Workload (one "step" = one full solve):
   * lattice 32x32x32x64, antiperiodic in t, smooth SU(3) links
     U = exp(i eps H), eps = 0.25, reunitarised (seeded, generated on the GPU
     by the library's own generator);
   * source: complex normal N(0,1) per component (seeded);
-  * kappa = 0.1303, as close to the critical point as the plain FP64
-    BiCGSTAB still converges on this field (620 iterations; at 0.1304 it
-    does not converge within 4000);
+  * kappa = 0.1303, as close to the critical point as plain FP64 BiCGSTAB
+    still converges on this field (865-870 iterations; at 0.1304 it does not
+    converge within 4000);
   * stop at a true relative residual ||b - M x|| / ||b|| <= 1e-10, recomputed
     in FP64 on the full two-parity system at the end of every solve.
-Timed: the chosen solver (FP64 flexible GCR around an FP32-spinor /
-16-bit-link inner BiCGSTAB run as a CUDA graph with a device-side loop).  The
-plain FP64 BiCGSTAB on the same GPU, the dslash bandwidth and a CPU baseline
-(the FP64 CPU oracle, all host cores, bounded sample) are reported beside it.
+Timed (`value`): the chosen solver -- FP64 flexible GCR(4) around an inner
+BiCGSTAB on 16-bit fixed-point spinors and 16-bit links with FP32
+arithmetic, run as one CUDA graph with a device-side WHILE loop per outer
+step.  Reported beside it: plain FP64 BiCGSTAB on the same GPU (this source
+and four more), the hopping-term bandwidth per storage and its roofline, the
+end-to-end time through the C ABI from host buffers, the clover target
+(32^3 x 64, csw 1, near-critical kappa), the 24^3 x 48 clover workload at
+every storage precision with errors against the CPU oracle's FP64 solve, the
+learned preconditioner, the batched multi-RHS solve, and a CPU baseline (the
+FP64 CPU oracle on all host cores, bounded sample).
+
+`--impl reference` times one complete FP64 solve of the CPU restatement of
+qcu's algorithm on the same system, measured, beside qcu's own GPU kernels
+rebuilt for sm_100a (its wilson_dslash kernel time, a full dslashQcu call,
+ncclBistabCgQcu).
 
 Multi-GPU: the path does not shard in this implementation (replicas only):
 every rank solves its own seeded system; the time is the max over ranks.
@@ -38,9 +49,7 @@ EPS = 0.25
 T_BC = -1.0
 GAUGE_SEED = 20251203
 SRC_SEED = 7
-KAPPA = 0.1303            # plain FP64 BiCGSTAB: 620-870 iterations on this ensemble, by summation order (0.1304: no convergence in 4000)
-PLAIN_ITERS_REF = 865     # the CPU oracle's own FP64 BiCGSTAB: 865 iterations to 1e-10 on this system (run once
-                          # to the end: 358 s on 8 cores); the reference arm extrapolates its sample to it
+KAPPA = 0.1303            # plain FP64 BiCGSTAB: 865-870 iterations on this ensemble (0.1304: no convergence in 4000)
 TOL = 1e-10
 CSW = 1.0
 KAPPA_CLOVER = 0.1291     # clover csw = 1 on the same field: near-critical (plain FP64 ~1000 iterations)
@@ -199,14 +208,24 @@ def cpu_dslash_medians(latt):
     return {"unit": "ms per application (FP64, one parity)", **out}
 
 
-def reference_gpu(latt):
+def reference_gpu(latt, U, psi):
     """qcu's own CUDA code, built from its sources for sm_100a
-    (oracle/_ref/libqcu_ref.so), on this GPU: the full dslashQcu call
-    (including qcu's per-call setup and in-place layout permutations) at
-    `latt`, and ncclBistabCgQcu (its fixed kappa 0.125 and absolute 1e-9
-    criterion) on 16^3 x 32.  qcu prints a line per dslash; its output is
-    kept off this process's stdout.  None when the build or a GPU is absent."""
+    (oracle/_ref/libqcu_ref.so), on this GPU, fed with the oracle's seeded
+    fields through torch (this library is not loaded):
+      * its hopping kernel wilson_dslash (src/wilson_dslash.cu:9-245) at
+        `latt`, launched as qcu launches it and timed with CUDA events by
+        oracle/ref_timer.cu, with its output checked against the oracle;
+      * the full dslashQcu call (qcu's per-call set-up and in-place layout
+        permutations included) at `latt`;
+      * ncclBistabCgQcu (its fixed kappa 0.125 and absolute 1e-9 criterion) on
+        16^3 x 32.
+    qcu prints a line per dslash; its output is kept off this process's
+    stdout.  None when the build or a GPU is absent."""
     import ctypes
+
+    import numpy as np
+
+    import oracle as O
 
     path = os.path.join(ROOT, "oracle", "_ref", "libqcu_ref.so")
     try:
@@ -214,10 +233,18 @@ def reference_gpu(latt):
 
         if not (os.path.exists(path) and torch.cuda.is_available()):
             return None
-        import qcu_b200 as q
+
+        class Param(ctypes.Structure):
+            _fields_ = [("lattice_size", ctypes.c_int * 4)]
+
+        def param(v):
+            p = Param()
+            for i in range(4):
+                p.lattice_size[i] = v[i]
+            return p
 
         ref = ctypes.CDLL(path)
-        Pp, vp = ctypes.POINTER(q.QcuParam), ctypes.c_void_p
+        Pp, vp = ctypes.POINTER(Param), ctypes.c_void_p
         ref.dslashQcu.argtypes = [vp, vp, vp, Pp, ctypes.c_int]
         ref.dslashQcu.restype = None
         ref.ncclBistabCgQcu.argtypes = [vp, vp, vp, Pp, Pp]
@@ -228,34 +255,45 @@ def reference_gpu(latt):
         os.dup2(devnull, 1)
         try:
             out = {}
-            L = q.Layout(tuple(latt))
-            U = torch.empty(L.gauge, dtype=torch.complex128, device="cuda")
-            q.gauge_random(U, latt, 1, EPS, GAUGE_SEED)
-            psi = torch.empty(L.half, dtype=torch.complex128, device="cuda")
-            q.fermion_random(psi, psi.numel(), 0, SRC_SEED)
-            o = torch.empty_like(psi)
-            par = q.QcuParam(latt)
-            ref.dslashQcu(o.data_ptr(), psi.data_ptr(), U.data_ptr(), ctypes.byref(par), 0)
+            tag = "x".join(map(str, latt))
+            dU = torch.from_numpy(U).cuda()
+            dpsi = torch.from_numpy(psi).cuda()
+            o = torch.empty_like(dpsi)
+            if hasattr(ref, "qcu_ref_wilson_dslash_timed"):  # the event-timing harness linked into the build
+                tim = ref
+                tim.qcu_ref_wilson_dslash_timed.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                                            ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+                ms = ctypes.c_double(0)
+                lat = (ctypes.c_int * 4)(*latt)
+                rc = tim.qcu_ref_wilson_dslash_timed(o.data_ptr(), dpsi.data_ptr(), dU.data_ptr(), lat, 0, 20,
+                                                     ctypes.byref(ms))
+                if rc == 0:
+                    oref = O.dslash(psi, U, latt, 0, 1.0)
+                    err = float(np.linalg.norm(o.cpu().numpy() - oref) / np.linalg.norm(oref))
+                    vh = O.vh(latt)
+                    out["wilson_dslash_kernel"] = {
+                        "lattice": tag, "ms": round(ms.value, 4), "launch": "qcu's own: blocks of 32, one site per thread",
+                        "GBps_at_1152B_per_site": round(DSLASH_BYTES["64"] * vh / (ms.value * 1e-3) / 1e9, 1),
+                        "rel_err_vs_oracle": err}
+            par = param(latt)
+            ref.dslashQcu(o.data_ptr(), dpsi.data_ptr(), dU.data_ptr(), ctypes.byref(par), 0)
             ts = []
             for _ in range(3):
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
-                ref.dslashQcu(o.data_ptr(), psi.data_ptr(), U.data_ptr(), ctypes.byref(par), 0)
+                ref.dslashQcu(o.data_ptr(), dpsi.data_ptr(), dU.data_ptr(), ctypes.byref(par), 0)
                 torch.cuda.synchronize()
                 ts.append(time.perf_counter() - t0)
-            out["dslashQcu_call_ms_" + "x".join(map(str, latt))] = round(1e3 * min(ts), 2)
-            del U, psi, o
+            out["dslashQcu_call_ms_" + tag] = round(1e3 * min(ts), 2)
+            del dU, dpsi, o
             small = [16, 16, 16, 32]
-            Ls = q.Layout(tuple(small))
-            U = torch.empty(Ls.gauge, dtype=torch.complex128, device="cuda")
-            q.gauge_random(U, small, 1, EPS, GAUGE_SEED)
-            b = torch.empty(Ls.full, dtype=torch.complex128, device="cuda")
-            q.fermion_random(b, b.numel(), 0, SRC_SEED)
-            x = torch.zeros_like(b)
-            par, grid = q.QcuParam(small), q.QcuParam([1, 1, 1, 1])
+            dU = torch.from_numpy(O.gauge_smooth(small, EPS, GAUGE_SEED)).cuda()
+            db = torch.from_numpy(O.fermion_gauss(O.full_shape(small), SRC_SEED)).cuda()
+            x = torch.zeros_like(db)
+            par, grid = param(small), param([1, 1, 1, 1])
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            ref.ncclBistabCgQcu(x.data_ptr(), b.data_ptr(), U.data_ptr(), ctypes.byref(par), ctypes.byref(grid))
+            ref.ncclBistabCgQcu(x.data_ptr(), db.data_ptr(), dU.data_ptr(), ctypes.byref(par), ctypes.byref(grid))
             torch.cuda.synchronize()
             out["ncclBistabCgQcu_s_16x16x16x32_kappa0.125"] = round(time.perf_counter() - t0, 4)
             return out
@@ -294,30 +332,70 @@ def max_over_ranks(pg, v, device=None):
     return float(t.item())
 
 
-def run_reference(args, world, rank, pg):
-    """Reference arm: the CPU restatement of qcu's algorithm (FP64 BiCGSTAB,
-    OpenMP, all host threads) on a bounded sample of the same workload."""
-    if rank != 0:
-        return
+def cpu_full_solve(latt, kappa, U, b, tol=TOL):
+    """One complete FP64 even-odd BiCGSTAB solve of the CPU oracle (qcu's
+    algorithm, include/lattice_bistabcg.h:101-132,221-340; OpenMP on every
+    host thread) to a true relative residual <= tol of the full system,
+    recomputed with the oracle's FP64 operator; restarted from its own
+    iterate with a tighter target if the iterated residual met the target
+    but the true one did not.  Returns (seconds, iterations, true residual)."""
     import numpy as np
 
+    import oracle as O
+
+    t0 = time.perf_counter()
+    nb = np.linalg.norm(b)
+    x, its, t_in = None, 0, tol
+    for _ in range(4):
+        x, it, _ = O.solve_full(b, U, latt, kappa, x0=x, t_bc=T_BC, tol=t_in, maxiter=20000)
+        its += it
+        res = float(np.linalg.norm(b - O.mfull(x, U, latt, kappa, T_BC)) / nb)
+        if res <= tol:
+            break
+        t_in *= 0.5 * tol / res
+    return time.perf_counter() - t0, its, res
+
+
+def run_reference(args, world, rank, pg):
+    """Reference arm.  qcu's code for this path is GPU code only, with no CPU
+    implementation, and its solver is fixed to kappa 0.125 and an absolute
+    tolerance (include/define.h:67-69), so it cannot run this workload.  The
+    arm therefore times the CPU restatement of qcu's algorithm (FP64 even-odd
+    BiCGSTAB, OpenMP, all host threads) on the same system: ONE complete
+    solve to a 1e-10 true residual, measured, not extrapolated.  A complete
+    solve takes minutes, so it runs once whatever --steps says
+    (cpu_solves_run).  Beside it: qcu's own GPU kernels rebuilt for sm_100a
+    (reference_gpu), and the CPU oracle's hopping term."""
+    if rank != 0:
+        return
     import oracle as O
 
     latt = list(args.latt)
     U = O.gauge_smooth(latt, EPS, GAUGE_SEED)
     b = O.fermion_gauss(O.full_shape(latt), SRC_SEED)
-    cb = cpu_sample(latt, args.kappa, U, b, PLAIN_ITERS_REF, budget_s=max(5.0, 60.0 / max(args.steps + args.warmup, 1)))
-    extra = {"cpu_dslash": cpu_dslash_medians(latt)}
-    rg = reference_gpu(latt) if latt == LATT else None
+    threads = O.get_threads()
+    extra = {} if args.no_cpu else {"cpu_dslash": cpu_dslash_medians(latt)}
+    rg = reference_gpu(latt, U, b[1]) if latt == LATT else None
     if rg is not None:
         extra["reference_gpu"] = rg
-    line = {"metric": METRIC, "value": cb["value"], "unit": "s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["value"] * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic (seeded)",
+    if args.no_cpu:  # qcu's GPU timings only (profiling runs)
+        print(json.dumps({"impl": "reference", "reference_gpu": rg}), flush=True)
+        return
+    secs, its, res = cpu_full_solve(latt, args.kappa, U, b)
+    sample = (f"one complete FP64 BiCGSTAB solve of the CPU oracle on {'x'.join(map(str, latt))}, kappa {args.kappa}: "
+              f"{its} iterations, true residual {res:.2e}, {secs:.1f} s on {threads} host threads (measured)")
+    line = {"metric": METRIC, "value": round(secs, 3), "unit": "s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(secs * 1e3, 1),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded smooth SU(3) gauge, Gaussian source)",
             "config": {"workload": "wilson-bicgstab-32^3x64-smooth-eps0.25", "latt": latt, "kappa": args.kappa,
                        "tol": TOL, "t_boundary": T_BC},
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": cb["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "cpu_solves_run": 1,
+            "note": ("value = one complete CPU solve, measured; it runs once (about 2.5 min), not --steps times, so "
+                     "the arm ends within minutes"),
+            "cpu_solve": {"seconds": round(secs, 3), "iterations": its, "true_residual": res},
+            "cpu_baseline": {"value": round(secs, 3), "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": round(secs, 3), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             **extra}
     print(json.dumps(line), flush=True)
 
@@ -410,6 +488,173 @@ def batch_config(args, q, stream, chosen_kw):
             "plain_fp64_seconds_estimate": round(plain, 4),
             "speedup_vs_one_at_a_time": round(single / tb, 3),
             "speedup_vs_plain_fp64": round(plain / tb, 3)}
+
+
+def legacy_calls(q, latt):
+    """This library through qcu's own ABI, on the inputs reference_gpu gives
+    qcu (same generators and seeds): a dslashQcu call at `latt` and
+    ncclBistabCgQcu (kappa 0.125, absolute 1e-9) on 16^3 x 32, wall time of
+    each synchronous call."""
+    import torch
+
+    out = {}
+    L = q.Layout(tuple(latt))
+    U = torch.empty(L.gauge, dtype=torch.complex128, device="cuda")
+    q.gauge_random(U, latt, 1, EPS, GAUGE_SEED)
+    b = torch.empty(L.full, dtype=torch.complex128, device="cuda")
+    q.fermion_random(b, b.numel(), 0, SRC_SEED)
+    psi = b[1].contiguous()
+    o = torch.empty_like(psi)
+    par = q.QcuParam(latt)
+    q.dslashQcu(o, psi, U, par, 0)
+    ts = []
+    for _ in range(5):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        q.dslashQcu(o, psi, U, par, 0)
+        ts.append(time.perf_counter() - t0)
+    out["dslashQcu_call_ms_" + "x".join(map(str, latt))] = round(1e3 * min(ts), 3)
+    del U, b, psi, o
+    small = [16, 16, 16, 32]
+    Ls = q.Layout(tuple(small))
+    U = torch.empty(Ls.gauge, dtype=torch.complex128, device="cuda")
+    q.gauge_random(U, small, 1, EPS, GAUGE_SEED)
+    b = torch.empty(Ls.full, dtype=torch.complex128, device="cuda")
+    q.fermion_random(b, b.numel(), 0, SRC_SEED)
+    x = torch.zeros_like(b)
+    grid = q.QcuParam([1, 1, 1, 1])
+    q.ncclBistabCgQcu(x, b, U, q.QcuParam(small), grid)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    q.ncclBistabCgQcu(x, b, U, q.QcuParam(small), grid)
+    torch.cuda.synchronize()
+    out["ncclBistabCgQcu_s_16x16x16x32_kappa0.125"] = round(time.perf_counter() - t0, 4)
+    return out
+
+
+def sources_block(q, G, latt, kappa, stream, chosen_kw, n_src=4):
+    """Plain FP64 BiCGSTAB and the chosen solver on n_src more Gaussian
+    sources of the benchmark system (same field): one timed solve each (CUDA
+    events), with the iteration counts, so the speed-up rests on more than
+    one right-hand side of a near-critical system."""
+    import statistics
+
+    import torch
+
+    L = q.Layout(tuple(latt))
+    b = torch.empty(L.full, dtype=torch.complex128, device="cuda")
+    x = torch.empty_like(b)
+    rows = []
+    for i in range(n_src):
+        seed = SRC_SEED + 1000 + i
+        q.fermion_random(b, b.numel(), 0, seed)
+        tp, ip = event_time(stream, lambda: G.invert(x, b, kappa, tol=TOL, maxiter=20000, precision=64, delta=0.0))
+        tc, ic = event_time(stream, lambda: G.invert(x, b, kappa, tol=TOL, maxiter=20000, **chosen_kw))
+        rows.append({"source_seed": seed, "plain_fp64_s": round(tp, 4), "plain_iterations": ip["iterations"],
+                     "plain_status": ip["status"], "chosen_s": round(tc, 4), "chosen_iterations": ic["iterations"],
+                     "chosen_status": ic["status"], "chosen_true_residual": ic["true_residual"],
+                     "speedup": round(tp / tc, 3)})
+    sp = [r["speedup"] for r in rows]
+    return {"sources": rows, "speedup_median": round(statistics.median(sp), 3),
+            "speedup_min": round(min(sp), 3), "speedup_max": round(max(sp), 3),
+            "plain_fp64_s_median": round(statistics.median(r["plain_fp64_s"] for r in rows), 4),
+            "chosen_s_median": round(statistics.median(r["chosen_s"] for r in rows), 4)}
+
+
+def clover_c3_block(q, stream):
+    """The clover workload: 24^3 x 48, smooth links eps 0.3, csw 1, kappa
+    0.125, Gaussian source.  Each storage precision's solve (one timed solve
+    after a warm-up) with its solution's error against the FP64 CPU oracle's
+    solve of the same system (OpenMP, to a 1e-11 true residual)."""
+    import numpy as np
+    import torch
+
+    import oracle as O
+
+    latt, eps, kappa = [24, 24, 24, 48], 0.3, 0.125
+    U = O.gauge_smooth(latt, eps, GAUGE_SEED + 3)
+    b = O.fermion_gauss(O.full_shape(latt), SRC_SEED + 3)
+    A = [O.clover_build(U, latt, p, kappa * CSW) for p in (0, 1)]
+    Ainv = [O.clover_invert(a) for a in A]
+    t0 = time.perf_counter()
+    xo, it_o, _ = O.solve_full(b, U, latt, kappa, t_bc=T_BC, Ainv_e=Ainv[0], Ainv_o=Ainv[1], tol=1e-11,
+                               maxiter=20000)
+    t_oracle = time.perf_counter() - t0
+    res_o = float(np.linalg.norm(b - O.mfull(xo, U, latt, kappa, T_BC, True, A[0], A[1])) / np.linalg.norm(b))
+    del A, Ainv
+    gcr = dict(solver="gcr", inner_iters=96, inner_tol=0.05, gcr_k=4)
+    methods = [("plain FP64 BiCGSTAB", dict(precision=64, delta=0.0)),
+               ("BiCGSTAB FP32 storage, FP64 reliable updates", dict(precision=32, delta=0.1)),
+               ("BiCGSTAB 16-bit storage, FP64 reliable updates", dict(precision=16, delta=0.1)),
+               ("FP64 GCR, inner FP32 spinors / 16-bit links", dict(precision=32, gauge_precision=16, **gcr)),
+               ("FP64 GCR, inner 16-bit spinors and links", dict(precision=16, **gcr))]
+    dU, db = torch.from_numpy(U).cuda(), torch.from_numpy(b).cuda()
+    x = torch.empty_like(db)
+    xo_t = torch.from_numpy(xo).cuda()
+    rows = []
+    with q.Gauge(dU, latt, t_boundary=T_BC, clover_coeff=kappa * CSW) as G:
+        del dU
+        for name, kw in methods:
+            G.invert(x, db, kappa, tol=TOL, maxiter=20000, clover=True, **kw)
+            t, info = event_time(stream, lambda: G.invert(x, db, kappa, tol=TOL, maxiter=20000, clover=True, **kw))
+            err = float(torch.linalg.vector_norm(x - xo_t) / torch.linalg.vector_norm(xo_t))
+            rows.append({"method": name, "seconds": round(t, 4), "iterations": info["iterations"],
+                         "status": info["status"], "true_residual": info["true_residual"],
+                         "rel_err_vs_fp64_oracle_solve": err})
+    return {"workload": f"wilson-clover-csw{CSW}-24^3x48-smooth-eps{eps}", "kappa": kappa,
+            "oracle_solve": {"iterations": it_o, "true_residual": res_o, "seconds_cpu": round(t_oracle, 2),
+                             "cores": O.get_threads()},
+            "methods": rows}
+
+
+def learned_block(q, stream, chosen_kw, gauge, b, latt):
+    """The learned preconditioner: the network trained (by the library's own
+    forward/backward kernels and Adam) on ~2000 (residual, error) pairs from
+    plain FP64 clover solves on seeded 16^4 smooth fields (eps 0.25), then
+    applied inside the FP64 flexible GCR on the 32^3 x 64 clover target at
+    near-critical kappa (precond=2: network, then the inner BiCGSTAB on what
+    it leaves); the chosen solver without it beside it, same system."""
+    import torch
+
+    from qcu_b200 import learn
+
+    small = [16, 16, 16, 16]
+    Ls = q.Layout(tuple(small))
+    us = torch.empty(Ls.gauge, dtype=torch.complex128, device="cuda")
+    q.gauge_random(us, small, 1, EPS, 4242)
+    t0 = time.perf_counter()
+    with q.Gauge(us, small, t_boundary=T_BC, clover_coeff=KAPPA_CLOVER * CSW) as Gs:
+        r, e = learn.make_pairs(Gs, KAPPA_CLOVER, 48, [2, 4, 6, 8, 10, 12, 16, 20, 24, 28, 32, 40, 48, 56, 64, 80,
+                                                     96, 112, 128, 160], clover=True)
+        t_pairs = time.perf_counter() - t0
+        net = q.Network(seed=1, init_scale=0.01)
+        t0 = time.perf_counter()
+        losses = learn.train(net, Gs, r, e, 1500, 16, 3e-3)
+        t_train = time.perf_counter() - t0
+    npairs = int(r.shape[0])
+    del r, e, us
+    x = torch.empty_like(b)
+    with q.Gauge(gauge, latt, t_boundary=T_BC, clover_coeff=KAPPA_CLOVER * CSW) as G:
+        kw = dict(chosen_kw)
+        kw["solver"] = "gcr"
+        G.invert(x, b, KAPPA_CLOVER, tol=TOL, maxiter=20000, clover=True, **kw)
+        t_no, i_no = event_time(stream, lambda: G.invert(x, b, KAPPA_CLOVER, tol=TOL, maxiter=20000, clover=True,
+                                                           **kw))
+        G.invert(x, b, KAPPA_CLOVER, tol=TOL, maxiter=20000, clover=True, precond=2, nn=net, **kw)
+        t_nn, i_nn = event_time(stream, lambda: G.invert(x, b, KAPPA_CLOVER, tol=TOL, maxiter=20000, clover=True,
+                                                           precond=2, nn=net, **kw))
+    net.close()
+    return {"training": {"lattice": "16^4 clover csw 1, eps 0.25", "pairs": npairs, "pair_seconds": round(t_pairs, 2),
+                         "steps": 1500, "train_seconds": round(t_train, 2),
+                         "loss_first": round(float(sum(losses[:50]) / 50), 5),
+                         "loss_last": round(float(sum(losses[-50:]) / 50), 5)},
+            "target": f"32^3x64 clover csw {CSW}, kappa {KAPPA_CLOVER}",
+            "without_network": {"seconds": round(t_no, 4), "inner_iterations": i_no["iterations"],
+                                "outer_steps": i_no["reliable_updates"], "true_residual": i_no["true_residual"]},
+            "with_network": {"seconds": round(t_nn, 4), "inner_iterations": i_nn["iterations"],
+                             "outer_steps": i_nn["reliable_updates"], "true_residual": i_nn["true_residual"],
+                             "status": i_nn["status"], "fallback": i_nn["fallback"]},
+            "gain": round(t_no / t_nn, 3)}
 
 
 def run_ours(args, world, rank, local, pg):
@@ -538,7 +783,11 @@ def run_ours(args, world, rank, local, pg):
 
     extra = {}
     if not args.no_extra and latt == LATT:
+        extra["legacy_abi"] = legacy_calls(q, latt)
+        extra["more_sources"] = sources_block(q, G, latt, args.kappa, lib_stream, chosen_kw)
         extra["clover_target"] = clover_target(args, q, gauge, b, x, latt, lib_stream, chosen_kw)
+        extra["clover_24x24x24x48"] = clover_c3_block(q, lib_stream)
+        extra["learned"] = learned_block(q, lib_stream, chosen_kw, gauge, b, latt)
         extra["batch"] = batch_config(args, q, lib_stream, chosen_kw)
 
     cpu = None

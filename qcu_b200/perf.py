@@ -4,6 +4,7 @@
     python -m qcu_b200.perf solve  --precision 32 --gauge-precision 16
     python -m qcu_b200.perf batch  --csw 1.0 --kappa 0.128
     python -m qcu_b200.perf precisions
+    python -m qcu_b200.perf legacy --iters 20
 
 `dslash` applies the even-odd hopping term `iters` times (after 3 warm-up
 launches) on a seeded smooth gauge field and prints the time per launch and
@@ -14,7 +15,9 @@ solves, in one batched call, the 12 point sources of a propagator on the
 main lattice together with 4 Gaussian right-hand sides on each of
 16^3 x 32, 24^3 x 48 and a second gauge field of the main lattice, and
 prints the batched wall time next to the same 24 systems solved one at a
-time.  `precisions` solves one system (default: the benchmark's) with plain
+time.  `legacy` calls dslashQcu (qcu's ABI: PyQuda-layout complex128
+fields, one kernel per call) `iters` times and prints the wall time per
+synchronous call.  `precisions` solves one system (default: the benchmark's) with plain
 FP64 BiCGSTAB, BiCGSTAB with FP64 reliable updates at 32 and 16 bits, and
 the FP64 GCR around 32- and 16-bit inner solves, and states each solution's
 difference from the FP64 one.  Inputs are
@@ -45,7 +48,7 @@ def _gauge(latt, eps, seed, t_bc, csw=0.0, kappa=0.0):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["dslash", "solve", "batch", "precisions"])
+    ap.add_argument("what", choices=["dslash", "solve", "batch", "precisions", "legacy"])
     ap.add_argument("--latt", type=int, nargs=4, default=[32, 32, 32, 64])
     ap.add_argument("--eps", type=float, default=0.25)
     ap.add_argument("--seed", type=int, default=20251203)
@@ -82,6 +85,25 @@ def main(argv=None):
         return
     if a.what == "batch":
         _batch(a)
+        return
+    if a.what == "legacy":
+        L = q.Layout(tuple(a.latt))
+        u = torch.empty(L.gauge, dtype=torch.complex128, device="cuda")
+        q.gauge_random(u, a.latt, 1, a.eps, a.seed)
+        psi = torch.empty(L.half, dtype=torch.complex128, device="cuda")
+        q.fermion_random(psi, psi.numel(), 0, 7)
+        out = torch.empty_like(psi)
+        par = q.QcuParam(a.latt)
+        for i in range(3):
+            q.dslashQcu(out, psi, u, par, i & 1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(a.iters):
+            q.dslashQcu(out, psi, u, par, i & 1)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3 / a.iters
+        print(json.dumps({"call": "dslashQcu", "latt": a.latt, "ms_per_call": round(ms, 4),
+                          "GBps_at_1152B_per_site": round(1152 * L.vh / (ms * 1e-3) / 1e9, 1)}))
         return
     if a.what == "precisions":
         _precisions(a)
