@@ -16,17 +16,20 @@
 //   SOA32 : float4,  NC = 6: float4 j = 3 * q + c holds colour c of spins 2q
 //           and 2q + 1 as (re, re, im, im), the lane pairs of the paired FP32
 //           instructions (hop32.cuh)
-//   SOA16 : uint4,   NC = 3  + float norm[Vh]: 16-bit fixed point
+//   SOA16 : 12 words per site + float norm[Vh]: 16-bit fixed point
 //           (offset-binary 16-bit, value/norm * 32767) scaled by the per-site max |component|;
 //           word k = 6 q + 2 c + (re, im) holds spin 2q (low half) and 2q + 1 (high
-//           half) of colour c, eight values per 16-byte load.  Fixed point keeps 15 bits of
-//           mantissa relative to the site maximum where FP16 keeps 11.
+//           half) of colour c.  A block of 32 sites is [32 x words 0-7][32 x words 8-11]
+//           (1024 + 512 B): one 32-byte and one 16-byte load per site.  Fixed point keeps
+//           15 bits of mantissa relative to the site maximum where FP16 keeps 11.
 // Gauge kinds (reconstruct-12: rows 0 and 1 stored, row 2 = conj(r0 x r1),
 // include/define.h:198-206), one slab of Vh_pad sites per (dir, parity):
 //   GAOS64 : PyQuda layout complex128 [dir][par][site][3][3], rows 0-1 read
 //   GSOA64 : double2, NC = 6
 //   GSOA32 : float4,  NC = 3
-//   GSOA16 : uint2,   NC = 3   (four 16-bit fixed point per load, |U_ij| <= 1)
+//   GSOA16 : 6 words per link (word e = element e of rows 0-1, 16-bit fixed point,
+//            |U_ij| <= 1); a block of 32 sites is [32 x words 0-3][32 x words 4-5]
+//            (512 + 256 B): one 16-byte and one 8-byte load per link
 #pragma once
 #include "cplx.cuh"
 
@@ -65,12 +68,62 @@ __device__ __forceinline__ unsigned fix16_pack_k(float a, float b, float k) {
   return __byte_perm(__float_as_uint(ra), __float_as_uint(rb), 0x5410);
 }
 
+// 256-bit global accesses (one request for 32 bytes; sm_100): p 32-byte aligned
+__device__ __forceinline__ void ldg256(const void *p, unsigned (&w)[8]) {
+  asm("ld.global.nc.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+      : "l"(p));
+}
+__device__ __forceinline__ void stg256(void *p, const unsigned (&w)[8]) {
+  asm volatile("st.global.v8.u32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "r"(w[0]), "r"(w[1]), "r"(w[2]),
+               "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7])
+               : "memory");
+}
+
 // site-blocked indexing
 constexpr int SB = 32;
 __host__ __device__ __forceinline__ int pad_sites(int Vh) { return (Vh + SB - 1) / SB * SB; }
 template <int NC>
 __host__ __device__ __forceinline__ size_t blk_base(int s) {
   return (size_t)(s >> 5) * NC * SB + (s & (SB - 1));
+}
+
+// SOA16: the 12 words of site s (words 0-7 at w8, 8-11 at w4)
+constexpr int S16_BLOCK_BYTES = 32 * 48;
+__host__ __device__ __forceinline__ size_t s16_w8(int s) { return (size_t)(s >> 5) * S16_BLOCK_BYTES + (s & 31) * 32; }
+__host__ __device__ __forceinline__ size_t s16_w4(int s) {
+  return (size_t)(s >> 5) * S16_BLOCK_BYTES + 1024 + (s & 31) * 16;
+}
+__device__ __forceinline__ void s16_load_words(const void *base, int s, unsigned (&w)[12]) {
+  unsigned a[8];
+  ldg256(static_cast<const char *>(base) + s16_w8(s), a);
+  const uint4 b = __ldg(reinterpret_cast<const uint4 *>(static_cast<const char *>(base) + s16_w4(s)));
+#pragma unroll
+  for (int k = 0; k < 8; k++) w[k] = a[k];
+  w[8] = b.x;
+  w[9] = b.y;
+  w[10] = b.z;
+  w[11] = b.w;
+}
+__device__ __forceinline__ void s16_store_words(void *base, int s, const unsigned (&w)[12]) {
+  unsigned a[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) a[k] = w[k];
+  stg256(static_cast<char *>(base) + s16_w8(s), a);
+  *reinterpret_cast<uint4 *>(static_cast<char *>(base) + s16_w4(s)) = make_uint4(w[8], w[9], w[10], w[11]);
+}
+// GSOA16: the 6 words of the link of site s in a slab starting `slab_sites` sites in
+constexpr int G16_BLOCK_BYTES = 32 * 24;
+__device__ __forceinline__ void g16_load_words(const void *base, size_t slab_sites, int s, unsigned (&w)[6]) {
+  const char *blk = static_cast<const char *>(base) + slab_sites * 24 + (size_t)(s >> 5) * G16_BLOCK_BYTES;
+  const uint4 a = __ldg(reinterpret_cast<const uint4 *>(blk) + (s & 31));
+  const uint2 b = __ldg(reinterpret_cast<const uint2 *>(blk + 512) + (s & 31));
+  w[0] = a.x;
+  w[1] = a.y;
+  w[2] = a.z;
+  w[3] = a.w;
+  w[4] = b.x;
+  w[5] = b.y;
 }
 
 // Lattice geometry of one parity (half lattice).  Site index
@@ -115,17 +168,9 @@ __device__ __forceinline__ void spinor_load(const SpinorView<K> &v, int s, Cpx<T
       out[a + 3] = Cpx<T>((T)d.y, (T)d.w);
     }
   } else {
-    const uint4 *p = static_cast<const uint4 *>(v.p) + blk_base<3>(s);
     const float nrm = __ldg(v.norm + s) * (1.0f / FIX16_SCALE);
     unsigned w[12];
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      const uint4 d = __ldg(p + j * SB);
-      w[4 * j] = d.x;
-      w[4 * j + 1] = d.y;
-      w[4 * j + 2] = d.z;
-      w[4 * j + 3] = d.w;
-    }
+    s16_load_words(v.p, s, w);
 #pragma unroll
     for (int k = 0; k < 12; k++) {  // word k = 6 * (spin pair) + 2 * colour + (re, im)
       const float2 f = fix16_unpack(w[k]);
@@ -170,9 +215,7 @@ __device__ __forceinline__ void spinor_store(const SpinorView<K> &v, int s, cons
       w[q] = q % 2 == 0 ? fix16_pack_k((float)in[a].re, (float)in[a + 3].re, k)
                         : fix16_pack_k((float)in[a].im, (float)in[a + 3].im, k);
     }
-    uint4 *p = static_cast<uint4 *>(v.p) + blk_base<3>(s);
-#pragma unroll
-    for (int j = 0; j < 3; j++) p[j * SB] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
+    s16_store_words(v.p, s, w);
     v.norm[s] = mx;
   }
 }
@@ -217,16 +260,12 @@ __device__ __forceinline__ void link_load(const GaugeView<G> &u, int dir, int pa
       m[2 * k + 1] = Cpx<T>((T)d.z, (T)d.w);
     }
   } else {
-    const uint2 *p = static_cast<const uint2 *>(u.p) + slab * 3 + blk_base<3>(s);
+    unsigned w[6];
+    g16_load_words(u.p, slab, s, w);
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-      uint2 d = __ldg(p + k * SB);
-      unsigned w[2] = {d.x, d.y};
-#pragma unroll
-      for (int q = 0; q < 2; q++) {
-        const float2 f = fix16_unpack(w[q]);
-        m[2 * k + q] = Cpx<T>((T)(f.x * (1.0f / FIX16_SCALE)), (T)(f.y * (1.0f / FIX16_SCALE)));
-      }
+    for (int k = 0; k < 6; k++) {
+      const float2 f = fix16_unpack(w[k]);
+      m[k] = Cpx<T>((T)(f.x * (1.0f / FIX16_SCALE)), (T)(f.y * (1.0f / FIX16_SCALE)));
     }
   }
   m[6] = (m[1] * m[5] - m[2] * m[4]).conj();

@@ -179,11 +179,12 @@ __global__ void k_gauge_pack(int Vh, const double2 *__restrict__ in, void *out) 
       for (int k = 0; k < 3; k++)
         o[k * SB] = make_float4((float)v[2 * k].x, (float)v[2 * k].y, (float)v[2 * k + 1].x, (float)v[2 * k + 1].y);
     } else {
-      uint2 *o = static_cast<uint2 *>(out) + slab * 3 * Vp + blk_base<3>(s);
+      char *blk = static_cast<char *>(out) + slab * Vp * 24 + (int64_t)(s >> 5) * G16_BLOCK_BYTES;
+      unsigned w[6];
 #pragma unroll
-      for (int k = 0; k < 3; k++)
-        o[k * SB] = make_uint2(fix16_pack((float)v[2 * k].x, (float)v[2 * k].y),
-                               fix16_pack((float)v[2 * k + 1].x, (float)v[2 * k + 1].y));
+      for (int k = 0; k < 6; k++) w[k] = fix16_pack((float)v[k].x, (float)v[k].y);
+      reinterpret_cast<uint4 *>(blk)[s & 31] = make_uint4(w[0], w[1], w[2], w[3]);
+      reinterpret_cast<uint2 *>(blk + 512)[s & 31] = make_uint2(w[4], w[5]);
     }
   }
 }

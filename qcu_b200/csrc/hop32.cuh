@@ -143,16 +143,8 @@ __device__ __forceinline__ float2 fix16_unpack2(unsigned w) {
 // SOA16 site in units of norm/32767 (word k = 6 q + 2 c + (re, im) is the lane
 // pair of spins 2q, 2q + 1); returns the site norm.
 __device__ __forceinline__ float site16_load_raw(const SpinorView<SOA16> &v, int s, Site2 &o) {
-  const uint4 *p = static_cast<const uint4 *>(v.p) + blk_base<3>(s);
   unsigned w[12];
-#pragma unroll
-  for (int j = 0; j < 3; j++) {
-    const uint4 d = __ldg(p + j * SB);
-    w[4 * j] = d.x;
-    w[4 * j + 1] = d.y;
-    w[4 * j + 2] = d.z;
-    w[4 * j + 3] = d.w;
-  }
+  s16_load_words(v.p, s, w);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     o.up.re[c] = fix16_unpack2(w[2 * c]);
@@ -172,16 +164,8 @@ __device__ __forceinline__ float2 fix16_biased2(unsigned w) {
                      __int_as_float(__byte_perm(w, 0x4B000000u, 0x7632)));
 }
 __device__ __forceinline__ float site16_load_biased(const SpinorView<SOA16> &v, int s, Site2 &o) {
-  const uint4 *p = static_cast<const uint4 *>(v.p) + blk_base<3>(s);
   unsigned w[12];
-#pragma unroll
-  for (int j = 0; j < 3; j++) {
-    const uint4 d = __ldg(p + j * SB);
-    w[4 * j] = d.x;
-    w[4 * j + 1] = d.y;
-    w[4 * j + 2] = d.z;
-    w[4 * j + 3] = d.w;
-  }
+  s16_load_words(v.p, s, w);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     o.up.re[c] = fix16_biased2(w[2 * c]);
@@ -214,9 +198,7 @@ __device__ __forceinline__ void site16_store(const SpinorView<SOA16> &v, int s, 
     w[6 + 2 * c] = fix16_pack2(x.lo.re[c], k);
     w[6 + 2 * c + 1] = fix16_pack2(x.lo.im[c], k);
   }
-  uint4 *p = static_cast<uint4 *>(v.p) + blk_base<3>(s);
-#pragma unroll
-  for (int j = 0; j < 3; j++) p[j * SB] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
+  s16_store_words(v.p, s, w);
   v.norm[s] = mx;
 }
 
@@ -274,15 +256,13 @@ __device__ __forceinline__ float link2_load(const GaugeView<G> &u, int dir, int 
     return 1.0f;
   } else {
     static_assert(G == GSOA16, "FP32 hop: GSOA32 or GSOA16 links");
-    const uint2 *p = static_cast<const uint2 *>(u.p) + slab * 3 + blk_base<3>(s);
+    unsigned w[6];
+    g16_load_words(u.p, slab, s, w);
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const uint2 d = __ldg(p + k * SB);
-      const float2 a = fix16_unpack(d.x), b = fix16_unpack(d.y);
-      m.re[2 * k] = bc2(a.x);
-      m.im[2 * k] = bc2(a.y);
-      m.re[2 * k + 1] = bc2(b.x);
-      m.im[2 * k + 1] = bc2(b.y);
+    for (int k = 0; k < 6; k++) {
+      const float2 a = fix16_unpack(w[k]);
+      m.re[k] = bc2(a.x);
+      m.im[k] = bc2(a.y);
     }
     link2_row2(m, 1.0f / FIX16_SCALE);
     return 1.0f / FIX16_SCALE;

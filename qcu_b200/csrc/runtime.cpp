@@ -110,6 +110,8 @@ void Spinor::alloc(int k, int vh) {
   kind = k;
   Vh = vh;
   data.ensure(spinor_bytes(k, vh));
+  // 16-bit spinors are read and written with 32-byte accesses
+  require(reinterpret_cast<uintptr_t>(data.p) % 32 == 0, "spinor buffer is not 32-byte aligned");
   if (k == SOA16) norm.ensure(spinor_norm_bytes(k, vh));
 }
 
