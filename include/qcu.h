@@ -53,8 +53,10 @@ void dslashCloverQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam 
 void mpiDslashQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, int parity, QcuParam *grid);
 void mpiBistabCgQcu(void *gauge, QcuParam *param, QcuParam *grid);
 
-/* as dslashQcu; `grid` must be {1,1,1,1} (single GPU, periodic wrap in-kernel).
- * Replaces src/nccl_wilson_dslash.cu:3-19. */
+/* as dslashQcu on one GPU when `grid` is {1,1,1,1} (periodic wrap in-kernel);
+ * otherwise this rank's part of the dslash of the global lattice split over
+ * `grid` ranks, `param` being the local lattice (see qcuCommInit in
+ * qcu_ext.h).  Replaces src/nccl_wilson_dslash.cu:3-19. */
 void ncclDslashQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, int parity, QcuParam *grid);
 
 /* Solves M x = b, M = 1 - kappa D, kappa = 0.125 (include/define.h:69), by

@@ -166,6 +166,37 @@ int qcuFermionRandom(void *psi, long long n_complex, int kind, unsigned long lon
 int dslashCloverQcuNoAlloc(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, int parity);
 int qcuNoAllocMaxSites(void);
 
+/* ---- Several GPUs: ncclDslashQcu with grid != {1,1,1,1} (qcu's domain
+ * decomposition, src/nccl_wilson_dslash.cu:3-19, include/lattice_dslash.h:11-197).
+ * Every rank (one process per GPU) passes its local sub-lattice in PyQuda
+ * layout, `param` = the local lattice size (every extent even) and `grid` =
+ * ranks per direction; rank r sits at qcu's grid coordinate
+ * (include/lattice_set.h:89-95: t fastest, rank = ((gx*Gy+gy)*Gz+gz)*Gt+gt).
+ * Faces of half spinors are exchanged with NCCL point-to-point over a
+ * communicator made once per device: one rank calls qcuCommUniqueId, the id
+ * (128 bytes) reaches every rank by the launcher's own means (MPI, a
+ * torch.distributed broadcast, ...), then each rank calls qcuCommInit with
+ * its rank.  NCCL (libnccl.so.2) is loaded on first use. */
+int qcuCommUniqueId(void *id);
+int qcuCommInit(const void *id, int nranks, int rank);
+int qcuCommFree(void);
+/* this rank's plan: [nranks, rank, coord[4], fwd[4], bwd[4], face[4]] (22
+ * ints; face = sites of one parity on the face of each partitioned direction,
+ * 0 elsewhere); needs no GPU */
+int qcuDDPlan(const int latt[4], const int grid[4], int rank, int *plan);
+/* the face exchange this rank carries out, in order: n_ops entries of 5 ints
+ * (kind 0 send / 1 recv, direction, slot, peer rank, complex count); slot 0
+ * of a direction is the low face (sent to the backward rank, received from
+ * the forward one), slot 1 the high face (sent forward, received from
+ * backward); at most 16 entries; needs no GPU */
+int qcuDDSchedule(const int latt[4], const int grid[4], int rank, int *ops, int *n_ops);
+/* every rank of `grid` at once in this process on the current GPU, faces
+ * exchanged by device copies following each rank's schedule: the same
+ * kernels as ncclDslashQcu without a second GPU.  *_all hold the ranks'
+ * local fields back to back in rank order. */
+int qcuDslashDDEmulate(void *out_all, const void *in_all, const void *gauge_all, const int latt[4], int parity,
+                       const int grid[4]);
+
 /* Learned preconditioner: a gauge-equivariant parallel-transport network
  * approximating M_pc^{-1} on the odd sites.  Two layers, 4 -> 16 -> 4
  * colour-vector channels (12 complex -> 48 -> 12 per site); each layer sums

@@ -141,6 +141,12 @@ _lib.qcuInvertBatch.argtypes = [ctypes.POINTER(QcuBatchSystem), ctypes.c_int, ct
                                 ctypes.POINTER(QcuInvertResult), ctypes.POINTER(QcuBatchTune)]
 _lib.qcuBatchApplyMatPC.argtypes = [ctypes.POINTER(QcuBatchSystem), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.POINTER(QcuBatchTune), ctypes.c_void_p]
+_ip = ctypes.POINTER(ctypes.c_int)
+_lib.qcuCommUniqueId.argtypes = [ctypes.c_void_p]
+_lib.qcuCommInit.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+_lib.qcuDDPlan.argtypes = [_ip, _ip, ctypes.c_int, _ip]
+_lib.qcuDDSchedule.argtypes = [_ip, _ip, ctypes.c_int, _ip, _ip]
+_lib.qcuDslashDDEmulate.argtypes = [_vp, _vp, _vp, _ip, ctypes.c_int, _ip]
 _lib.qcuGaugeRandom.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong]
 _lib.qcuFermionRandom.argtypes = [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_ulonglong]
 _lib.qcuGetStream.restype = _vp
@@ -368,6 +374,73 @@ def batch_apply_matpc(systems, precision: int = 16, gauge_precision: int = 0, ds
     _check(_lib.qcuBatchApplyMatPC(sys_arr, len(systems), int(precision), int(gauge_precision), ctypes.byref(tune),
                                    dots.ctypes.data))
     return dots[:nrhs]
+
+
+# ---------------------------------------------------------------- several GPUs
+def _ivec(v, n=4):
+    if len(v) != n:
+        raise ValueError(f"expected {n} integers")
+    return (ctypes.c_int * n)(*[int(x) for x in v])
+
+
+def dd_plan(latt, grid, rank: int) -> dict:
+    """This rank's place in the grid (qcuDDPlan): coordinates, the
+    neighbouring ranks in each direction, and the face sizes (sites of one
+    parity) of the partitioned directions.  Needs no GPU."""
+    out = (ctypes.c_int * 22)()
+    _check(_lib.qcuDDPlan(_ivec(latt), _ivec(grid), int(rank), out))
+    v = list(out)
+    return {"nranks": v[0], "rank": v[1], "coord": v[2:6], "fwd": v[6:10], "bwd": v[10:14], "face": v[14:18]}
+
+
+def dd_schedule(latt, grid, rank: int):
+    """The face exchange this rank carries out, in order (qcuDDSchedule): a
+    list of (kind, direction, slot, peer, count) with kind "send" or "recv"
+    and count in complex numbers.  Needs no GPU."""
+    ops = (ctypes.c_int * 80)()
+    n = ctypes.c_int(0)
+    _check(_lib.qcuDDSchedule(_ivec(latt), _ivec(grid), int(rank), ops, ctypes.byref(n)))
+    v = list(ops)
+    return [(("send", "recv")[v[5 * i]], v[5 * i + 1], v[5 * i + 2], v[5 * i + 3], v[5 * i + 4])
+            for i in range(n.value)]
+
+
+def dslash_dd_emulate(out_all, in_all, gauge_all, latt, parity: int, grid) -> None:
+    """Every rank of `grid` in this process on the current GPU
+    (qcuDslashDDEmulate): *_all hold the ranks' local PyQuda-layout fields
+    back to back in rank order; latt is the local lattice."""
+    _check(_lib.qcuDslashDDEmulate(_ptr(out_all), _ptr(in_all), _ptr(gauge_all), _ivec(latt), int(parity),
+                                   _ivec(grid)))
+
+
+def comm_init(group=None) -> None:
+    """Set up this device's communicator for ncclDslashQcu with a grid of
+    ranks, from an initialised torch.distributed process group (any backend):
+    rank 0 makes the NCCL id, the group broadcasts it, every rank calls
+    qcuCommInit with its rank."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    buf = (ctypes.c_ubyte * 128)()
+    if rank == 0:
+        _check(_lib.qcuCommUniqueId(buf))
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.tensor(list(buf), dtype=torch.uint8, device=dev)
+    dist.broadcast(t, src=dist.get_global_rank(group, 0) if group is not None else 0, group=group)
+    ids = (ctypes.c_ubyte * 128)(*t.cpu().tolist())
+    _check(_lib.qcuCommInit(ids, world, rank))
+
+
+def comm_unique_id() -> bytes:
+    """A fresh NCCL unique id (qcuCommUniqueId), 128 bytes."""
+    buf = (ctypes.c_ubyte * 128)()
+    _check(_lib.qcuCommUniqueId(buf))
+    return bytes(buf)
+
+
+def comm_free() -> None:
+    _check(_lib.qcuCommFree())
 
 
 def point_sources(latt, origin, device="cuda"):

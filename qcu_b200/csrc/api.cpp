@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "batch.h"
+#include "dd.h"
 #include "nn.h"
 #include "solver.h"
 
@@ -52,6 +53,12 @@ static void check_grid(const QcuParam *grid) {
     require(grid->lattice_size[d] == 1,
             "this implementation runs on one GPU: grid must be {1,1,1,1}");
 }
+static bool single_rank(const QcuParam *grid) {
+  require(grid != nullptr, "grid pointer is null");
+  for (int d = 0; d < 4; d++)
+    if (grid->lattice_size[d] != 1) return false;
+  return true;
+}
 
 static int legacy_dslash_call(void *out, void *in, void *gauge, QcuParam *param, int parity, int clover) {
   QCU_API_BEGIN
@@ -76,13 +83,23 @@ void mpiBistabCgQcu(void *, QcuParam *, QcuParam *) {}
 
 void ncclDslashQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, int parity, QcuParam *grid) {
   clear_last_error();
+  bool one = true;
   try {
-    check_grid(grid);
+    one = single_rank(grid);
+    if (!one) {
+      // this rank's sub-lattice; faces exchanged with the neighbouring ranks
+      // over the communicator set up by qcuCommInit (src/nccl_wilson_dslash.cu:3-19)
+      require(param != nullptr, "param pointer is null");
+      dd_dslash_nccl(fermion_out, fermion_in, gauge, param->lattice_size, parity, grid->lattice_size);
+    }
   } catch (const qcu::Error &e) {
     set_last_error(e.code, e.what());
     return;
+  } catch (const std::exception &e) {
+    set_last_error(3, e.what());
+    return;
   }
-  legacy_dslash_call(fermion_out, fermion_in, gauge, param, parity, 0);
+  if (one) legacy_dslash_call(fermion_out, fermion_in, gauge, param, parity, 0);
 }
 
 void ncclBistabCgQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, QcuParam *grid) {
@@ -303,6 +320,60 @@ int dslashCloverQcuNoAlloc(void *fermion_out, void *fermion_in, void *gauge, Qcu
 }
 
 int qcuNoAllocMaxSites(void) { return noalloc_max_vh(); }
+
+int qcuCommUniqueId(void *id) {
+  QCU_API_BEGIN
+  dd_unique_id(id);
+  QCU_API_END
+}
+
+int qcuCommInit(const void *id, int nranks, int rank) {
+  QCU_API_BEGIN
+  dd_comm_init(id, nranks, rank);
+  QCU_API_END
+}
+
+int qcuCommFree(void) {
+  QCU_API_BEGIN
+  dd_comm_free();
+  QCU_API_END
+}
+
+int qcuDDPlan(const int latt[4], const int grid[4], int rank, int *plan) {
+  QCU_API_BEGIN
+  require(plan != nullptr, "null plan buffer");
+  const DDPlan p = dd_plan(latt, grid, rank);
+  int k = 0;
+  plan[k++] = p.nranks;
+  plan[k++] = p.rank;
+  for (int d = 0; d < 4; d++) plan[k++] = p.coord[d];
+  for (int d = 0; d < 4; d++) plan[k++] = p.fwd[d];
+  for (int d = 0; d < 4; d++) plan[k++] = p.bwd[d];
+  for (int d = 0; d < 4; d++) plan[k++] = p.face[d];
+  QCU_API_END
+}
+
+int qcuDDSchedule(const int latt[4], const int grid[4], int rank, int *ops, int *n_ops) {
+  QCU_API_BEGIN
+  require(ops != nullptr && n_ops != nullptr, "null schedule buffer");
+  const std::vector<DDOp> s = dd_schedule(dd_plan(latt, grid, rank));
+  for (size_t i = 0; i < s.size(); i++) {
+    ops[5 * i] = s[i].kind;
+    ops[5 * i + 1] = s[i].dir;
+    ops[5 * i + 2] = s[i].slot;
+    ops[5 * i + 3] = s[i].peer;
+    ops[5 * i + 4] = s[i].count;
+  }
+  *n_ops = (int)s.size();
+  QCU_API_END
+}
+
+int qcuDslashDDEmulate(void *out_all, const void *in_all, const void *gauge_all, const int latt[4], int parity,
+                       const int grid[4]) {
+  QCU_API_BEGIN
+  dd_dslash_emulate(out_all, in_all, gauge_all, latt, parity, grid);
+  QCU_API_END
+}
 
 int qcuNNCreate(qcuNN *net, unsigned long long seed, double init_scale) {
   QCU_API_BEGIN
