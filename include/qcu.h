@@ -63,8 +63,9 @@ void ncclDslashQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam *p
  * even-odd preconditioned BiCGSTAB from a uniform random initial guess, until
  * the iterated ||r_o||^2 < 1e-9 or 1000 iterations (include/define.h:67-68,
  * include/lattice_bistabcg.h:221-340).  fermion_out = x, fermion_in = b, both
- * full spinors; `grid` must be {1,1,1,1}.  Replaces
- * src/nccl_wilson_bistabcg.cu:7-27. */
+ * full spinors; with `grid` != {1,1,1,1}, this rank's part of the solve on the
+ * global lattice split over the grid (param = the local lattice; see
+ * qcuCommInit in qcu_ext.h).  Replaces src/nccl_wilson_bistabcg.cu:7-27. */
 void ncclBistabCgQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam *param, QcuParam *grid);
 
 #ifdef __cplusplus

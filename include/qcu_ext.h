@@ -196,6 +196,14 @@ int qcuDDSchedule(const int latt[4], const int grid[4], int rank, int *ops, int 
  * local fields back to back in rank order. */
 int qcuDslashDDEmulate(void *out_all, const void *in_all, const void *gauge_all, const int latt[4], int parity,
                        const int grid[4]);
+/* ncclBistabCgQcu's solve over `grid` for every rank at once in this process
+ * (full spinors and gauges back to back in rank order): qcu's kappa 0.125,
+ * random start (seed 23333, each element fixed by its global site, so the
+ * start equals the single-GPU one on the global lattice) and stop on the
+ * grid-wide iterated ||r_o||^2 < 1e-9 or 1000 iterations.  Reports the
+ * iterations and the final ||r_o||^2. */
+int qcuBistabCgDDEmulate(void *x_all, const void *b_all, const void *gauge_all, const int latt[4], const int grid[4],
+                         int *iterations, double *r2);
 
 /* Learned preconditioner: a gauge-equivariant parallel-transport network
  * approximating M_pc^{-1} on the odd sites.  Two layers, 4 -> 16 -> 4

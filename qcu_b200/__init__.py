@@ -147,6 +147,7 @@ _lib.qcuCommInit.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
 _lib.qcuDDPlan.argtypes = [_ip, _ip, ctypes.c_int, _ip]
 _lib.qcuDDSchedule.argtypes = [_ip, _ip, ctypes.c_int, _ip, _ip]
 _lib.qcuDslashDDEmulate.argtypes = [_vp, _vp, _vp, _ip, ctypes.c_int, _ip]
+_lib.qcuBistabCgDDEmulate.argtypes = [_vp, _vp, _vp, _ip, _ip, _ip, ctypes.POINTER(ctypes.c_double)]
 _lib.qcuGaugeRandom.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong]
 _lib.qcuFermionRandom.argtypes = [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_ulonglong]
 _lib.qcuGetStream.restype = _vp
@@ -411,6 +412,16 @@ def dslash_dd_emulate(out_all, in_all, gauge_all, latt, parity: int, grid) -> No
     back to back in rank order; latt is the local lattice."""
     _check(_lib.qcuDslashDDEmulate(_ptr(out_all), _ptr(in_all), _ptr(gauge_all), _ivec(latt), int(parity),
                                    _ivec(grid)))
+
+
+def bistabcg_dd_emulate(x_all, b_all, gauge_all, latt, grid):
+    """ncclBistabCgQcu's solve over `grid` for every rank at once in this
+    process (qcuBistabCgDDEmulate); returns (iterations, final ||r_o||^2)."""
+    it = ctypes.c_int(0)
+    r2 = ctypes.c_double(0)
+    _check(_lib.qcuBistabCgDDEmulate(_ptr(x_all), _ptr(b_all), _ptr(gauge_all), _ivec(latt), _ivec(grid),
+                                     ctypes.byref(it), ctypes.byref(r2)))
+    return it.value, r2.value
 
 
 def comm_init(group=None) -> None:

@@ -47,12 +47,6 @@ struct qcuNN_s {
     return 3;                                      \
   }
 
-static void check_grid(const QcuParam *grid) {
-  require(grid != nullptr, "grid pointer is null");
-  for (int d = 0; d < 4; d++)
-    require(grid->lattice_size[d] == 1,
-            "this implementation runs on one GPU: grid must be {1,1,1,1}");
-}
 static bool single_rank(const QcuParam *grid) {
   require(grid != nullptr, "grid pointer is null");
   for (int d = 0; d < 4; d++)
@@ -107,7 +101,13 @@ void ncclBistabCgQcu(void *fermion_out, void *fermion_in, void *gauge, QcuParam 
   GaugeHandle *G = nullptr;
   try {
     require(param != nullptr, "param pointer is null");
-    check_grid(grid);
+    if (!single_rank(grid)) {
+      // this rank's part of the solve over the grid: qcu's kappa, start,
+      // criterion and iteration cap, inner products summed over all ranks
+      dd_solve(fermion_out, fermion_in, gauge, param->lattice_size, grid->lattice_size, false, 0.125, 1e-9, 1000,
+               23333);
+      return;
+    }
     G = gauge_load(gauge, param->lattice_size, 1.0, 0.0);
     SolveParams p;
     p.kappa = 0.125;   // include/define.h:69
@@ -372,6 +372,15 @@ int qcuDslashDDEmulate(void *out_all, const void *in_all, const void *gauge_all,
                        const int grid[4]) {
   QCU_API_BEGIN
   dd_dslash_emulate(out_all, in_all, gauge_all, latt, parity, grid);
+  QCU_API_END
+}
+
+int qcuBistabCgDDEmulate(void *x_all, const void *b_all, const void *gauge_all, const int latt[4], const int grid[4],
+                         int *iterations, double *r2) {
+  QCU_API_BEGIN
+  const DDSolveResult r = dd_solve(x_all, b_all, gauge_all, latt, grid, true, 0.125, 1e-9, 1000, 23333);
+  if (iterations) *iterations = r.iterations;
+  if (r2) *r2 = r.r2;
   QCU_API_END
 }
 

@@ -42,6 +42,7 @@
 #include <vector>
 
 #include "dd.h"
+#include "rng.cuh"
 
 namespace qcu {
 
@@ -292,7 +293,57 @@ __global__ void __launch_bounds__(DSLASH_BLOCK, 3)
   spinor_store<AOS64, double>(SpinorView<AOS64>{out, nullptr, g.Vh}, s, acc);
 }
 
-// ---------------------------------------------------------------- host: buffers and launches
+// ---------------------------------------------------------------- vector kernels of the distributed solver
+// out = a x + b y + c z on n complex numbers (y, z optional); out may alias any input
+__global__ void k_dd_lin3(int64_t n, double2 *out, double2 a, const double2 *x, double2 b, const double2 *y,
+                          double2 c, const double2 *z) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const Cpx<double> xa(x[i].x, x[i].y);
+    Cpx<double> v = Cpx<double>(a.x, a.y) * xa;
+    if (y) v += Cpx<double>(b.x, b.y) * Cpx<double>(y[i].x, y[i].y);
+    if (z) v += Cpx<double>(c.x, c.y) * Cpx<double>(z[i].x, z[i].y);
+    out[i] = make_double2(v.re, v.im);
+  }
+}
+// block partials of Re<a,b>, Im<a,b>, |a|^2 (<a,b> = sum conj(a) b)
+constexpr int DD_RED_BLOCK = 256;
+__global__ void __launch_bounds__(DD_RED_BLOCK) k_dd_dots(int64_t n, const double2 *a, const double2 *b, double *part) {
+  double v[3] = {0, 0, 0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 x = a[i], y = b[i];
+    v[0] += x.x * y.x + x.y * y.y;
+    v[1] += x.x * y.y - x.y * y.x;
+    v[2] += x.x * x.x + x.y * x.y;
+  }
+  __shared__ double sh[3][DD_RED_BLOCK];
+  for (int k = 0; k < 3; k++) sh[k][threadIdx.x] = v[k];
+  __syncthreads();
+  for (int w = DD_RED_BLOCK / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int k = 0; k < 3; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; k++) part[blockIdx.x * 3 + k] = sh[k][0];
+}
+// qcu's random start on the odd sites (include/lattice_bistabcg.h:108-109),
+// the value of each element fixed by its GLOBAL site: element (global odd
+// half-index G, component c) uses counters 2(12 G + c) and 2(12 G + c) + 1 --
+// the same field as the single-GPU solver's start on the global lattice
+__global__ void k_dd_uniform_odd(DDDev d, double2 *x, uint64_t seed, int4 origin, int4 glatt) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= d.g.Vh) return;
+  const Coord c = dd_coord(d.g, s, 1);
+  const int64_t X = origin.x + c.x, Y = origin.y + c.y, Z = origin.z + c.z, T = origin.w + c.t;
+  const int64_t G = ((T * glatt.z + Z) * glatt.y + Y) * (glatt.x / 2) + (X >> 1);
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    const uint64_t e = (uint64_t)G * 12 + k;
+    x[(size_t)s * 12 + k] = make_double2(rng_uniform(seed, 2 * e), rng_uniform(seed, 2 * e + 1));
+  }
+}
+
+// ---------------------------------------------------------------- host: one or all ranks of a grid
 namespace {
 // face buffers of one rank: send[d][0..1], halo[d][0..1]
 struct DDBufs {
@@ -327,76 +378,6 @@ struct DDSpace {
   }
 };
 
-void launch_pack(const DDDev &d, const void *in, const void *gauge, int par, cudaStream_t s) {
-  k_dd_pack<<<(d.g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK, DSLASH_BLOCK, 0, s>>>(d, static_cast<const double2 *>(in),
-                                                                               gauge, par);
-  QCU_CHECK_LAUNCH();
-}
-void launch_dd_dslash(const DDDev &d, const void *in, const void *gauge, void *out, int par, cudaStream_t s) {
-  k_dd_dslash<<<(d.g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK, DSLASH_BLOCK, 0, s>>>(
-      d, static_cast<const double2 *>(in), gauge, static_cast<double2 *>(out), par);
-  QCU_CHECK_LAUNCH();
-}
-}  // namespace
-
-void dd_dslash_emulate(void *out_all, const void *in_all, const void *gauge_all, const int latt[4], int parity,
-                       const int grid[4]) {
-  require(out_all && in_all && gauge_all, "dd: null pointer argument");
-  require(parity == 0 || parity == 1, "parity must be 0 or 1");
-  const DDPlan p0 = dd_plan(latt, grid, 0);
-  const Geom g = make_geom(latt);
-  Context &ctx = context();
-  std::lock_guard<std::mutex> lk(ctx.mu);
-  DDSpace &sp = per_device<DDSpace>(ctx);
-  const cudaStream_t st = ctx.stream;
-  const size_t half = (size_t)g.Vh * 12 * sizeof(double2), gauge_sz = (size_t)g.Vh * 8 * 9 * sizeof(double2);
-  auto in_of = [&](int r) { return static_cast<const char *>(in_all) + half * r; };
-  auto out_of = [&](int r) { return static_cast<char *>(out_all) + half * r; };
-  auto gauge_of = [&](int r) { return static_cast<const char *>(gauge_all) + gauge_sz * r; };
-  QCU_CUDA(cudaDeviceSynchronize());
-  std::vector<DDPlan> plans;
-  for (int r = 0; r < p0.nranks; r++) {
-    plans.push_back(dd_plan(latt, grid, r));
-    sp.at(r).ensure(plans[r]);
-  }
-  for (int r = 0; r < p0.nranks; r++)
-    launch_pack(sp.at(r).dev(plans[r], g), in_of(r), gauge_of(r), 1 - parity, st);
-  // the exchange schedule of every rank, carried out as device copies: a send
-  // of rank r to peer q is matched with q's next receive from r
-  std::vector<std::vector<DDOp>> sched;
-  for (int r = 0; r < p0.nranks; r++) sched.push_back(dd_schedule(plans[r]));
-  std::vector<std::vector<int>> next_recv(p0.nranks, std::vector<int>(p0.nranks, 0));
-  for (int r = 0; r < p0.nranks; r++) {
-    for (const DDOp &op : sched[r]) {
-      if (op.kind != DD_SEND) continue;
-      const int q = op.peer;
-      // q's receives from r, in q's order
-      int seen = 0, idx = -1;
-      for (size_t k = 0; k < sched[q].size(); k++) {
-        const DDOp &o = sched[q][k];
-        if (o.kind == DD_RECV && o.peer == r) {
-          if (seen == next_recv[q][r]) {
-            idx = (int)k;
-            break;
-          }
-          seen++;
-        }
-      }
-      require(idx >= 0, "dd: exchange schedule has a send without a matching receive");
-      next_recv[q][r]++;
-      const DDOp &rv = sched[q][idx];
-      require(rv.count == op.count, "dd: send and receive sizes differ");
-      QCU_CUDA(cudaMemcpyAsync(sp.at(q).halo[rv.dir][rv.slot].p, sp.at(r).send[op.dir][op.slot].p,
-                               (size_t)op.count * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-    }
-  }
-  for (int r = 0; r < p0.nranks; r++)
-    launch_dd_dslash(sp.at(r).dev(plans[r], g), in_of(r), gauge_of(r), out_of(r), parity, st);
-  QCU_CUDA(cudaStreamSynchronize(st));
-}
-
-// ---------------------------------------------------------------- NCCL
-namespace {
 struct NcclApi {
   void *lib = nullptr;
   ncclResult_t (*getUniqueId)(ncclUniqueId *) = nullptr;
@@ -404,6 +385,8 @@ struct NcclApi {
   ncclResult_t (*commDestroy)(ncclComm_t) = nullptr;
   ncclResult_t (*send)(const void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
   ncclResult_t (*recv)(void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*allReduce)(const void *, void *, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t,
+                            cudaStream_t) = nullptr;
   ncclResult_t (*groupStart)() = nullptr;
   ncclResult_t (*groupEnd)() = nullptr;
   const char *(*errorString)(ncclResult_t) = nullptr;
@@ -426,6 +409,7 @@ NcclApi &nccl() {
   api.commDestroy = reinterpret_cast<decltype(api.commDestroy)>(sym("ncclCommDestroy"));
   api.send = reinterpret_cast<decltype(api.send)>(sym("ncclSend"));
   api.recv = reinterpret_cast<decltype(api.recv)>(sym("ncclRecv"));
+  api.allReduce = reinterpret_cast<decltype(api.allReduce)>(sym("ncclAllReduce"));
   api.groupStart = reinterpret_cast<decltype(api.groupStart)>(sym("ncclGroupStart"));
   api.groupEnd = reinterpret_cast<decltype(api.groupEnd)>(sym("ncclGroupEnd"));
   api.errorString = reinterpret_cast<decltype(api.errorString)>(sym("ncclGetErrorString"));
@@ -440,7 +424,314 @@ struct DDComm {
   int nranks = 0, rank = -1;
 };
 DDComm &comm_of(const Context &ctx) { return per_device<DDComm>(ctx); }
+
+// The distributed operators on this process's ranks: every rank of the grid
+// (emulated, faces exchanged by device copies) or this process's one rank
+// (faces exchanged with NCCL).  The caller holds the context lock.
+class DDRun {
+ public:
+  DDRun(Context &ctx, const int latt[4], const int grid[4], bool emulate)
+      : ctx_(ctx), g_(make_geom(latt)), emulate_(emulate) {
+    DDSpace &sp = per_device<DDSpace>(ctx);
+    if (emulate) {
+      const int n = dd_plan(latt, grid, 0).nranks;
+      for (int r = 0; r < n; r++) plans_.push_back(dd_plan(latt, grid, r));
+    } else {
+      DDComm &c = comm_of(ctx);
+      require(c.comm != nullptr,
+              "ncclDslashQcu/ncclBistabCgQcu with grid != {1,1,1,1}: no communicator on this device (qcuCommInit)");
+      plans_.push_back(dd_plan(latt, grid, c.rank));
+      require(plans_[0].nranks == c.nranks, "dd: the grid's rank count differs from the communicator's");
+      comm_ = c.comm;
+    }
+    for (size_t r = 0; r < plans_.size(); r++) {
+      sp.at((int)r).ensure(plans_[r]);
+      dev_.push_back(sp.at((int)r).dev(plans_[r], g_));
+      bufs_.push_back(&sp.at((int)r));
+    }
+  }
+  int domains() const { return (int)plans_.size(); }
+  const Geom &geom() const { return g_; }
+  const DDPlan &plan(int r) const { return plans_[r]; }
+  const DDDev &dev(int r) const { return dev_[r]; }
+
+  // out[r] = D_{par <- 1-par} in[r] on every domain (PyQuda-layout halves)
+  void dslash(int par, const std::vector<const void *> &gauge, const std::vector<const void *> &in,
+              const std::vector<void *> &out) {
+    const cudaStream_t st = ctx_.stream;
+    for (int r = 0; r < domains(); r++) launch_pack(dev_[r], in[r], gauge[r], 1 - par, st);
+    exchange();
+    for (int r = 0; r < domains(); r++) launch_dd_dslash(dev_[r], in[r], gauge[r], out[r], par, st);
+  }
+
+  // v[0..n) summed over all ranks of the grid (over the domains of this
+  // process when emulating, then across processes with NCCL); v holds this
+  // process's per-domain values, domain-major: v[d * n + k]
+  void allsum(std::vector<double> &v, int n) {
+    std::vector<double> tot(n, 0.0);
+    for (int r = 0; r < domains(); r++)
+      for (int k = 0; k < n; k++) tot[k] += v[(size_t)r * n + k];
+    if (!emulate_) {
+      red_.ensure(n * sizeof(double));
+      QCU_CUDA(cudaMemcpyAsync(red_.p, tot.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx_.stream));
+      nccl_check(nccl().allReduce(red_.p, red_.p, n, ncclDouble, ncclSum, comm_, ctx_.stream), "ncclAllReduce");
+      QCU_CUDA(cudaMemcpyAsync(tot.data(), red_.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx_.stream));
+      QCU_CUDA(cudaStreamSynchronize(ctx_.stream));
+    }
+    v = tot;
+  }
+
+ private:
+  void exchange() {
+    const cudaStream_t st = ctx_.stream;
+    if (!emulate_) {
+      NcclApi &n = nccl();
+      const std::vector<DDOp> ops = dd_schedule(plans_[0]);
+      DDBufs &b = *bufs_[0];
+      nccl_check(n.groupStart(), "ncclGroupStart");
+      for (const DDOp &op : ops) {
+        const size_t cnt = (size_t)op.count * 2;  // complex128 as pairs of doubles
+        if (op.kind == DD_SEND)
+          nccl_check(n.send(b.send[op.dir][op.slot].p, cnt, ncclDouble, op.peer, comm_, st), "ncclSend");
+        else
+          nccl_check(n.recv(b.halo[op.dir][op.slot].p, cnt, ncclDouble, op.peer, comm_, st), "ncclRecv");
+      }
+      nccl_check(n.groupEnd(), "ncclGroupEnd");
+      return;
+    }
+    // every rank's schedule carried out as device copies: a send of rank r to
+    // peer q is matched with q's next receive from r
+    const int n = domains();
+    std::vector<std::vector<DDOp>> sched;
+    for (int r = 0; r < n; r++) sched.push_back(dd_schedule(plans_[r]));
+    std::vector<std::vector<int>> next_recv(n, std::vector<int>(n, 0));
+    for (int r = 0; r < n; r++) {
+      for (const DDOp &op : sched[r]) {
+        if (op.kind != DD_SEND) continue;
+        const int q = op.peer;
+        int seen = 0, idx = -1;
+        for (size_t k = 0; k < sched[q].size(); k++) {
+          const DDOp &o = sched[q][k];
+          if (o.kind == DD_RECV && o.peer == r) {
+            if (seen == next_recv[q][r]) {
+              idx = (int)k;
+              break;
+            }
+            seen++;
+          }
+        }
+        require(idx >= 0, "dd: exchange schedule has a send without a matching receive");
+        next_recv[q][r]++;
+        const DDOp &rv = sched[q][idx];
+        require(rv.count == op.count, "dd: send and receive sizes differ");
+        QCU_CUDA(cudaMemcpyAsync(bufs_[q]->halo[rv.dir][rv.slot].p, bufs_[r]->send[op.dir][op.slot].p,
+                                 (size_t)op.count * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+      }
+    }
+  }
+  static void launch_pack(const DDDev &d, const void *in, const void *gauge, int par, cudaStream_t s) {
+    k_dd_pack<<<(d.g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK, DSLASH_BLOCK, 0, s>>>(
+        d, static_cast<const double2 *>(in), gauge, par);
+    QCU_CHECK_LAUNCH();
+  }
+  static void launch_dd_dslash(const DDDev &d, const void *in, const void *gauge, void *out, int par,
+                               cudaStream_t s) {
+    k_dd_dslash<<<(d.g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK, DSLASH_BLOCK, 0, s>>>(
+        d, static_cast<const double2 *>(in), gauge, static_cast<double2 *>(out), par);
+    QCU_CHECK_LAUNCH();
+  }
+
+  Context &ctx_;
+  Geom g_;
+  bool emulate_;
+  ncclComm_t comm_ = nullptr;
+  std::vector<DDPlan> plans_;
+  std::vector<DDDev> dev_;
+  std::vector<DDBufs *> bufs_;
+  DevBuf red_;
+};
+
+std::vector<const void *> split_c(const void *all, size_t bytes, int n) {
+  std::vector<const void *> v;
+  for (int r = 0; r < n; r++) v.push_back(static_cast<const char *>(all) + bytes * r);
+  return v;
+}
+std::vector<void *> split(void *all, size_t bytes, int n) {
+  std::vector<void *> v;
+  for (int r = 0; r < n; r++) v.push_back(static_cast<char *>(all) + bytes * r);
+  return v;
+}
+
+// qcu's solver on the grid (include/lattice_bistabcg.h:101-132,221-340):
+// b'_o = b_o + kappa D_oe b_e; BiCGSTAB on M_pc = 1 - kappa^2 D_oe D_eo from
+// qcu's random start until the iterated, grid-wide ||r||^2 < tol (absolute)
+// or maxiter iterations; x_e = b_e + kappa D_eo x_o.  Scalars and inner
+// products are formed on the host from every rank's sums.
+DDSolveResult dd_bicgstab(DDRun &run, const std::vector<const void *> &gauge, const std::vector<void *> &x,
+                          const std::vector<const void *> &b, double kappa, double tol, int maxiter, uint64_t seed,
+                          const int glatt[4]) {
+  const Geom &g = run.geom();
+  const int R = run.domains();
+  const int64_t n = (int64_t)g.Vh * 12;
+  const size_t half = (size_t)n * sizeof(double2);
+  Context &ctx = context();
+  const cudaStream_t st = ctx.stream;
+  // per domain: b', r, rt, p, v, s, t, tmp, x_o
+  enum { BP, RR, RT, PP, VV, SS, TT, TMP, XO, NV };
+  std::vector<std::vector<std::unique_ptr<DevBuf>>> w(R);
+  for (int r = 0; r < R; r++)
+    for (int k = 0; k < NV; k++) {
+      w[r].push_back(std::make_unique<DevBuf>());
+      w[r][k]->ensure(half);
+    }
+  auto V = [&](int k) {
+    std::vector<void *> v;
+    for (int r = 0; r < R; r++) v.push_back(w[r][k]->p);
+    return v;
+  };
+  auto VC = [&](int k) {
+    std::vector<const void *> v;
+    for (int r = 0; r < R; r++) v.push_back(w[r][k]->p);
+    return v;
+  };
+  const int grid_blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+  auto lin3 = [&](int r, void *out, Cpx<double> a, const void *xx, Cpx<double> bb = {0, 0}, const void *y = nullptr,
+                  Cpx<double> c = {0, 0}, const void *z = nullptr) {
+    k_dd_lin3<<<grid_blocks, 256, 0, st>>>(n, static_cast<double2 *>(out), make_double2(a.re, a.im),
+                                           static_cast<const double2 *>(xx), make_double2(bb.re, bb.im),
+                                           static_cast<const double2 *>(y), make_double2(c.re, c.im),
+                                           static_cast<const double2 *>(z));
+    QCU_CHECK_LAUNCH();
+  };
+  DevBuf part;
+  part.ensure((size_t)grid_blocks * 3 * sizeof(double));
+  std::vector<double> ph((size_t)grid_blocks * 3);
+  // grid-wide Re<a,b>, Im<a,b>, |a|^2
+  auto dots = [&](int ka, int kb) {
+    std::vector<double> v((size_t)R * 3, 0.0);
+    for (int r = 0; r < R; r++) {
+      k_dd_dots<<<grid_blocks, DD_RED_BLOCK, 0, st>>>(n, static_cast<const double2 *>(w[r][ka]->p),
+                                                     static_cast<const double2 *>(w[r][kb]->p), part.as<double>());
+      QCU_CHECK_LAUNCH();
+      QCU_CUDA(cudaMemcpyAsync(ph.data(), part.p, ph.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+      QCU_CUDA(cudaStreamSynchronize(st));
+      for (int i = 0; i < grid_blocks; i++)
+        for (int k = 0; k < 3; k++) v[(size_t)r * 3 + k] += ph[(size_t)i * 3 + k];
+    }
+    run.allsum(v, 3);
+    return v;
+  };
+  const double k2 = kappa * kappa;
+  // out = M_pc in = in - kappa^2 D_oe D_eo in
+  auto mpc = [&](int kin, int kout) {
+    run.dslash(0, gauge, VC(kin), V(TMP));
+    run.dslash(1, gauge, VC(TMP), V(kout));
+    for (int r = 0; r < R; r++) lin3(r, w[r][kout]->p, {-k2, 0}, w[r][kout]->p, {1, 0}, w[r][kin]->p);
+  };
+  std::vector<const void *> be, bo;
+  std::vector<void *> xe, xo_out;
+  for (int r = 0; r < R; r++) {
+    be.push_back(b[r]);
+    bo.push_back(static_cast<const char *>(b[r]) + half);
+    xe.push_back(x[r]);
+    xo_out.push_back(static_cast<char *>(x[r]) + half);
+  }
+  // b'_o = b_o + kappa D_oe b_e
+  run.dslash(1, gauge, be, V(TMP));
+  for (int r = 0; r < R; r++) lin3(r, w[r][BP]->p, {1, 0}, bo[r], {kappa, 0}, w[r][TMP]->p);
+  // random start
+  for (int r = 0; r < R; r++) {
+    const DDPlan &p = run.plan(r);
+    const int4 origin = make_int4(p.coord[0] * p.latt[0], p.coord[1] * p.latt[1], p.coord[2] * p.latt[2],
+                                  p.coord[3] * p.latt[3]);
+    k_dd_uniform_odd<<<(g.Vh + 127) / 128, 128, 0, st>>>(run.dev(r), static_cast<double2 *>(w[r][XO]->p), seed,
+                                                          origin, make_int4(glatt[0], glatt[1], glatt[2], glatt[3]));
+    QCU_CHECK_LAUNCH();
+  }
+  mpc(XO, VV);
+  for (int r = 0; r < R; r++) {
+    lin3(r, w[r][RR]->p, {1, 0}, w[r][BP]->p, {-1, 0}, w[r][VV]->p);
+    QCU_CUDA(cudaMemcpyAsync(w[r][RT]->p, w[r][RR]->p, half, cudaMemcpyDeviceToDevice, st));
+    QCU_CUDA(cudaMemsetAsync(w[r][PP]->p, 0, half, st));
+    QCU_CUDA(cudaMemsetAsync(w[r][VV]->p, 0, half, st));
+  }
+  Cpx<double> rho(1, 0), alpha(1, 0), omega(1, 0);
+  DDSolveResult res;
+  res.r2 = dots(RR, RR)[2];
+  for (int it = 0; it < maxiter && !(res.r2 < tol); it++) {
+    std::vector<double> d = dots(RT, RR);
+    const Cpx<double> rho_n(d[0], d[1]);
+    const Cpx<double> beta = cdiv(rho_n, rho) * cdiv(alpha, omega);
+    rho = rho_n;
+    for (int r = 0; r < R; r++)  // p = r + beta (p - omega v)
+      lin3(r, w[r][PP]->p, {1, 0}, w[r][RR]->p, beta, w[r][PP]->p, Cpx<double>(0, 0) - beta * omega, w[r][VV]->p);
+    mpc(PP, VV);
+    d = dots(RT, VV);
+    alpha = cdiv(rho, Cpx<double>(d[0], d[1]));
+    for (int r = 0; r < R; r++) lin3(r, w[r][SS]->p, {1, 0}, w[r][RR]->p, Cpx<double>(0, 0) - alpha, w[r][VV]->p);
+    mpc(SS, TT);
+    d = dots(TT, SS);
+    omega = Cpx<double>(d[0] / d[2], d[1] / d[2]);
+    for (int r = 0; r < R; r++) {
+      lin3(r, w[r][XO]->p, {1, 0}, w[r][XO]->p, alpha, w[r][PP]->p, omega, w[r][SS]->p);
+      lin3(r, w[r][RR]->p, {1, 0}, w[r][SS]->p, Cpx<double>(0, 0) - omega, w[r][TT]->p);
+    }
+    res.r2 = dots(RR, RR)[2];
+    res.iterations = it + 1;
+    require(res.r2 == res.r2, "dd: the solve produced a non-finite residual");
+  }
+  // x_o, and x_e = b_e + kappa D_eo x_o
+  run.dslash(0, gauge, VC(XO), V(TMP));
+  for (int r = 0; r < R; r++) {
+    QCU_CUDA(cudaMemcpyAsync(xo_out[r], w[r][XO]->p, half, cudaMemcpyDeviceToDevice, st));
+    lin3(r, xe[r], {1, 0}, be[r], {kappa, 0}, w[r][TMP]->p);
+  }
+  QCU_CUDA(cudaStreamSynchronize(st));
+  return res;
+}
 }  // namespace
+
+void dd_dslash_emulate(void *out_all, const void *in_all, const void *gauge_all, const int latt[4], int parity,
+                       const int grid[4]) {
+  require(out_all && in_all && gauge_all, "dd: null pointer argument");
+  require(parity == 0 || parity == 1, "parity must be 0 or 1");
+  Context &ctx = context();
+  std::lock_guard<std::mutex> lk(ctx.mu);
+  DDRun run(ctx, latt, grid, true);
+  const Geom &g = run.geom();
+  const int n = run.domains();
+  const size_t half = (size_t)g.Vh * 12 * sizeof(double2), gauge_sz = (size_t)g.Vh * 8 * 9 * sizeof(double2);
+  QCU_CUDA(cudaDeviceSynchronize());
+  run.dslash(parity, split_c(gauge_all, gauge_sz, n), split_c(in_all, half, n), split(out_all, half, n));
+  QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+void dd_dslash_nccl(void *out, const void *in, const void *gauge, const int latt[4], int parity, const int grid[4]) {
+  require(out && in && gauge, "dslash: null pointer argument");
+  require(parity == 0 || parity == 1, "parity must be 0 or 1");
+  Context &ctx = context();
+  std::lock_guard<std::mutex> lk(ctx.mu);
+  DDRun run(ctx, latt, grid, false);
+  QCU_CUDA(cudaDeviceSynchronize());
+  run.dslash(parity, {gauge}, {in}, {out});
+  QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+DDSolveResult dd_solve(void *x, const void *b, const void *gauge, const int latt[4], const int grid[4], bool emulate,
+                       double kappa, double tol, int maxiter, uint64_t seed) {
+  require(x && b && gauge, "solve: null pointer argument");
+  Context &ctx = context();
+  std::lock_guard<std::mutex> lk(ctx.mu);
+  DDRun run(ctx, latt, grid, emulate);
+  const Geom &g = run.geom();
+  const int n = run.domains();
+  const size_t full = (size_t)g.Vh * 24 * sizeof(double2), gauge_sz = (size_t)g.Vh * 8 * 9 * sizeof(double2);
+  int glatt[4];
+  for (int d = 0; d < 4; d++) glatt[d] = latt[d] * grid[d];
+  QCU_CUDA(cudaDeviceSynchronize());
+  return dd_bicgstab(run, split_c(gauge, gauge_sz, n), split(x, full, n), split_c(b, full, n), kappa, tol, maxiter,
+                     seed, glatt);
+}
 
 void dd_unique_id(void *id) {
   require(id != nullptr, "dd: null id buffer");
@@ -468,35 +759,6 @@ void dd_comm_free() {
   DDComm &c = comm_of(ctx);
   if (c.comm) nccl().commDestroy(c.comm);
   c = DDComm();
-}
-
-void dd_dslash_nccl(void *out, const void *in, const void *gauge, const int latt[4], int parity, const int grid[4]) {
-  require(out && in && gauge, "dslash: null pointer argument");
-  require(parity == 0 || parity == 1, "parity must be 0 or 1");
-  Context &ctx = context();
-  std::lock_guard<std::mutex> lk(ctx.mu);
-  DDComm &c = comm_of(ctx);
-  require(c.comm != nullptr, "ncclDslashQcu with grid != {1,1,1,1}: no communicator on this device (qcuCommInit)");
-  const DDPlan p = dd_plan(latt, grid, c.rank);
-  require(p.nranks == c.nranks, "ncclDslashQcu: the grid's rank count differs from the communicator's");
-  const Geom g = make_geom(latt);
-  DDBufs &b = per_device<DDSpace>(ctx).at(0);
-  b.ensure(p);
-  const DDDev dv = b.dev(p, g);
-  const cudaStream_t st = ctx.stream;
-  QCU_CUDA(cudaDeviceSynchronize());
-  launch_pack(dv, in, gauge, 1 - parity, st);
-  const std::vector<DDOp> ops = dd_schedule(p);
-  NcclApi &n = nccl();
-  nccl_check(n.groupStart(), "ncclGroupStart");
-  for (const DDOp &op : ops) {
-    const size_t cnt = (size_t)op.count * 2;  // complex128 as pairs of doubles
-    if (op.kind == DD_SEND) nccl_check(n.send(b.send[op.dir][op.slot].p, cnt, ncclDouble, op.peer, c.comm, st), "ncclSend");
-    else nccl_check(n.recv(b.halo[op.dir][op.slot].p, cnt, ncclDouble, op.peer, c.comm, st), "ncclRecv");
-  }
-  nccl_check(n.groupEnd(), "ncclGroupEnd");
-  launch_dd_dslash(dv, in, gauge, out, parity, st);
-  QCU_CUDA(cudaStreamSynchronize(st));
 }
 
 }  // namespace qcu

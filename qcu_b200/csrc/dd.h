@@ -42,6 +42,15 @@ void dd_dslash_emulate(void *out_all, const void *in_all, const void *gauge_all,
                        const int grid[4]);
 // this rank's part, faces exchanged with NCCL over the device's communicator
 void dd_dslash_nccl(void *out, const void *in, const void *gauge, const int latt[4], int parity, const int grid[4]);
+// qcu's solver (ncclBistabCgQcu) on the grid: x, b full spinors of every
+// domain of this process (all ranks when emulating, back to back), stop on
+// the grid-wide iterated ||r_o||^2 < tol (absolute) or maxiter
+struct DDSolveResult {
+  int iterations = 0;
+  double r2 = 0;
+};
+DDSolveResult dd_solve(void *x, const void *b, const void *gauge, const int latt[4], const int grid[4], bool emulate,
+                       double kappa, double tol, int maxiter, uint64_t seed);
 void dd_unique_id(void *id);  // 128 bytes
 void dd_comm_init(const void *id, int nranks, int rank);
 void dd_comm_free();

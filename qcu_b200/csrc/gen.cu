@@ -8,21 +8,10 @@
 // initial guess (src/lattice_cuda.cu:3-14); this project does not reproduce
 // cuRAND's streams.
 #include "internal.h"
+#include "rng.cuh"
 
 namespace qcu {
 
-__host__ __device__ __forceinline__ uint64_t sm64_mix(uint64_t z) {
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-  return z ^ (z >> 31);
-}
-__host__ __device__ __forceinline__ uint64_t rng_u64(uint64_t seed, uint64_t ctr) {
-  const uint64_t s = sm64_mix(seed + 0x9E3779B97F4A7C15ULL);
-  return sm64_mix(s + (ctr + 1) * 0x9E3779B97F4A7C15ULL);
-}
-__device__ __forceinline__ double rng_uniform(uint64_t seed, uint64_t ctr) {
-  return (double)((rng_u64(seed, ctr) >> 11) + 1) * (1.0 / 9007199254740992.0);
-}
 __device__ __forceinline__ Cpx<double> rng_cgauss(uint64_t seed, uint64_t k) {
   const double u1 = rng_uniform(seed, 2 * k), u2 = rng_uniform(seed, 2 * k + 1);
   const double r = sqrt(-2.0 * log(u1));

@@ -87,3 +87,28 @@ def test_nccl_path_setup_and_checks(q):
     q.ncclDslashQcu(out, psi, U, q.QcuParam(loc), 0, q.QcuParam([1, 1, 1, 1]))
     assert q.last_error()[0] == 0
     assert rel(host(out), O.dslash(host(psi), host(U), loc, 0)) <= 1e-13
+
+
+@pytest.mark.parametrize("grid,loc", [([2, 1, 1, 1], [4, 4, 4, 4]), ([1, 1, 2, 2], [4, 4, 4, 4]),
+                                      ([1, 2, 1, 1], [4, 4, 4, 8])], ids=lambda v: "x".join(map(str, v)))
+def test_dd_bistabcg_equals_global(q, grid, loc):
+    """ncclBistabCgQcu over a grid (every rank emulated in this process):
+    qcu's contract (kappa 0.125, random start, grid-wide ||r_o||^2 < 1e-9);
+    the gathered solution solves the oracle's global system to that bound
+    and agrees with the single-GPU solve of the global lattice, which starts
+    from the same field."""
+    glatt = [loc[d] * grid[d] for d in range(4)]
+    U = O.gauge_smooth(glatt, 0.25, 71)
+    b = O.fermion_gauss(O.full_shape(glatt), 72)
+    xl = empty_like_dev((int(np.prod(grid)), 2) + tuple(O.half_shape(loc)))
+    it, r2 = q.bistabcg_dd_emulate(xl, dev(scatter_spinor(b, glatt, loc, grid)),
+                                   dev(scatter_gauge(U, glatt, loc, grid)), loc, grid)
+    assert 0 < it < 1000 and r2 < 1e-9
+    xh = host(xl)
+    x = np.stack([gather_half(np.ascontiguousarray(xh[:, p]), p, glatt, loc, grid) for p in (0, 1)])
+    r = b - O.mfull(x, U, glatt, 0.125)
+    assert np.linalg.norm(r) ** 2 < 1.1e-9
+    x1 = empty_like_dev(O.full_shape(glatt))
+    q.ncclBistabCgQcu(x1, dev(b), dev(U), q.QcuParam(glatt), q.QcuParam([1, 1, 1, 1]))
+    assert q.last_error()[0] == 0
+    assert rel(x, host(x1)) < 1e-6
