@@ -218,8 +218,13 @@ int qcuNNFree(qcuNN net);
 int qcuNNNumParams(void);
 int qcuNNGetWeights(qcuNN net, float *w);
 int qcuNNSetWeights(qcuNN net, const float *w);
-/* out = N(in) on odd-parity half spinors (complex128 PyQuda layout) */
+/* out = N(in) on odd-parity half spinors (complex128 PyQuda layout).
+ * Inference (this call and the GCR preconditioner) runs each layer's channel
+ * mixing on the tensor cores: tcgen05 BF16 MMAs with FP32 accumulators in
+ * tensor memory, the parallel transports rounded to bf16 as the A operand;
+ * qcuNNSetTensorCores(net, 0) selects the FP32 FMA layers instead. */
 int qcuNNApply(qcuNN net, qcuGauge h, void *out, const void *in);
+int qcuNNSetTensorCores(qcuNN net, int on);
 /* One training step on a batch of (residual r_i, error e_i) odd half spinors
  * ([batch][Vh][4][3] complex128): loss = mean_i |N(r_i) - e_i|^2 / |e_i|^2,
  * gradients by the hand-written backward kernels, then an Adam step with

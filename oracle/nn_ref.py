@@ -80,24 +80,36 @@ class Lattice:
         return v * self.ph_b[mu, p][None, :, None, None]
 
 
-def layer(lat, W, f, out_parities):
-    """one parallel-transport layer; returns [B, 2, Vh, Cout, 3] (zero on other parities)"""
+def bf16_round_complex(z):
+    """real and imaginary parts rounded to bfloat16, as the tensor-core layer's A operand"""
+    z = np.asarray(z, complex)
+    return bf16_round(z.real.astype(np.float32)).astype(np.float64) + 1j * bf16_round(
+        z.imag.astype(np.float32)).astype(np.float64)
+
+
+def layer(lat, W, f, out_parities, round_act=False):
+    """one parallel-transport layer; returns [B, 2, Vh, Cout, 3] (zero on other parities).
+    round_act: the transported inputs rounded to bf16 before the channel
+    mixing (the tensor-core layer, whose MMA operands are bf16)."""
     B = f.shape[0]
     out = np.zeros((B, 2, lat.Vh, W.shape[1], 3), complex)
     for p in out_parities:
         for h in range(HOPS):
-            out[:, p] += np.einsum("ab,nsbx->nsax", W[h], lat.transport(f, h, p))
+            v = lat.transport(f, h, p)
+            if round_act:
+                v = bf16_round_complex(v)
+            out[:, p] += np.einsum("ab,nsbx->nsax", W[h], v)
     return out
 
 
-def forward(lat, w, r_odd):
+def forward(lat, w, r_odd, round_act=False):
     """N(r) for odd half spinors r [B, Vh, 4, 3] -> (output odd [B, Vh, 4, 3], hidden)"""
     w1, w2 = split_weights(w)
     B = r_odd.shape[0]
     f0 = np.zeros((B, 2, lat.Vh, C_IN, 3), complex)
     f0[:, 1] = r_odd
-    hid = layer(lat, w1, f0, (0, 1))
-    out = layer(lat, w2, hid, (1,))
+    hid = layer(lat, w1, f0, (0, 1), round_act)
+    out = layer(lat, w2, hid, (1,), round_act)
     return out[:, 1], hid, f0
 
 

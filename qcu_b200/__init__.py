@@ -161,6 +161,7 @@ _lib.qcuNNNumParams.restype = ctypes.c_int
 _lib.qcuNNGetWeights.argtypes = [_vp, ctypes.c_void_p]
 _lib.qcuNNSetWeights.argtypes = [_vp, ctypes.c_void_p]
 _lib.qcuNNApply.argtypes = [_vp, _vp, _vp, _vp]
+_lib.qcuNNSetTensorCores.argtypes = [_vp, ctypes.c_int]
 _lib.qcuNNTrainStep.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
                                 ctypes.c_void_p]
 _lib.qcuBenchDslash.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -556,6 +557,10 @@ class Network:
 
     def apply(self, gauge: "Gauge", out, inp):
         _check(_lib.qcuNNApply(self._h, gauge._h, _ptr(out), _ptr(inp)))
+
+    def set_tensor_cores(self, on: bool):
+        """Inference on the tcgen05 tensor-core layers (default) or the FP32 FMA ones."""
+        _check(_lib.qcuNNSetTensorCores(self._h, int(bool(on))))
 
     def train_step(self, gauge: "Gauge", r, e, batch: int, lr: float, want_grad: bool = False):
         """Returns (loss, grad or None); r, e: [batch][Vh][4][3] complex128 device buffers."""

@@ -416,6 +416,13 @@ int qcuNNSetWeights(qcuNN net, const float *w) {
   QCU_API_END
 }
 
+int qcuNNSetTensorCores(qcuNN net, int on) {
+  QCU_API_BEGIN
+  require(net != nullptr, "null network");
+  nn_set_tensor_cores(*net->n, on);
+  QCU_API_END
+}
+
 int qcuNNApply(qcuNN net, qcuGauge h, void *out, const void *in) {
   QCU_API_BEGIN
   require(net && h && out && in, "null argument");

@@ -35,6 +35,10 @@ struct PtcArgs {
 
 // forward (or adjoint) layer; cin/cout in {4, 16}
 void launch_ptc(int cin, int cout, const Geom &g, const PtcArgs &a, cudaStream_t s);
+// the forward layer with bf16 weights on the tensor cores (nn_tc.cu): the
+// transported inputs are rounded to bf16, accumulation is FP32; err is set
+// to 1 if a wait of the kernel timed out
+void launch_ptc_tc(int cin, int cout, const Geom &g, const PtcArgs &a, int *err, int sms, cudaStream_t s);
 
 // grad[h][a][b] += sum_x sum_colour delta_a(x) conj((T_h in_b)(x)), over the
 // output parities in a.out_mask (a.out holds delta).  grad: [9][cout][cin] complex FP32.
@@ -66,5 +70,9 @@ void nn_apply_pyq(NNet &n, const GaugeHandle &G, void *out, const void *in);
 double nn_train_step(NNet &n, const GaugeHandle &G, const void *r, const void *e, int B, double lr, float *grad_host);
 void nn_apply_soa64(NNet &n, const GaugeHandle &G, const void *r64, void *z64, cudaStream_t s);
 void nn_prepare(NNet &n, int Vh);
+// throws if a tensor-core layer of the network reported a timed-out wait
+void nn_check(NNet &n);
+// 1: inference runs the tensor-core layers (default); 0: the FMA layers
+void nn_set_tensor_cores(NNet &n, int on);
 
 }  // namespace qcu

@@ -20,6 +20,8 @@ constexpr int NN_NPARAM = 2 * (NN_W1 + NN_W2);        // reals
 struct NNet {
   DevBuf w, w16, m, v, grad;       // FP32 master, bf16 copy, Adam moments, gradient
   DevBuf in, hid, out, delta2, delta1, target, enorm, loss;  // work fields (grown to batch x lattice)
+  DevBuf err;   // set by the tensor-core layers if a wait timed out
+  int tensor_cores = 1;
   int step = 0;
   int batch_cap = 0, vh_cap = 0;
   float2 *w1() const { return w.as<float2>(); }
@@ -52,6 +54,8 @@ NNet *nn_create(uint64_t seed, double scale) {
   auto *n = new NNet();
   n->w.ensure(NN_NPARAM * sizeof(float));
   n->w16.ensure(NN_NPARAM / 2 * sizeof(uint32_t));
+  n->err.ensure(sizeof(int));
+  QCU_CUDA(cudaMemset(n->err.p, 0, sizeof(int)));
   n->m.ensure(NN_NPARAM * sizeof(float));
   n->v.ensure(NN_NPARAM * sizeof(float));
   n->grad.ensure(NN_NPARAM * sizeof(float));
@@ -101,7 +105,10 @@ static void forward(NNet &n, const GaugeHandle &G, int B, bool bf16, cudaStream_
   a.out_mask = 3;
   if (bf16) a.w16 = n.w16_1();
   else a.w = n.w1();
-  launch_ptc(NN_C_IN, NN_C_HID, G.g, a, s);
+  const bool tc = bf16 && n.tensor_cores;
+  Context &ctx = context();
+  if (tc) launch_ptc_tc(NN_C_IN, NN_C_HID, G.g, a, n.err.as<int>(), ctx.sms, s);
+  else launch_ptc(NN_C_IN, NN_C_HID, G.g, a, s);
   PtcArgs b2 = a;
   b2.in = n.hid.as<float2>();
   b2.out = n.out.as<float2>();
@@ -111,8 +118,20 @@ static void forward(NNet &n, const GaugeHandle &G, int B, bool bf16, cudaStream_
   b2.w16 = nullptr;
   if (bf16) b2.w16 = n.w16_2();
   else b2.w = n.w2();
-  launch_ptc(NN_C_HID, NN_C_OUT, G.g, b2, s);
+  if (tc) launch_ptc_tc(NN_C_HID, NN_C_OUT, G.g, b2, n.err.as<int>(), ctx.sms, s);
+  else launch_ptc(NN_C_HID, NN_C_OUT, G.g, b2, s);
 }
+
+void nn_check(NNet &n) {
+  int e = 0;
+  QCU_CUDA(cudaMemcpy(&e, n.err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    QCU_CUDA(cudaMemset(n.err.p, 0, sizeof(int)));
+    throw Error(2, "network: a tensor-core layer timed out waiting for its MMAs");
+  }
+}
+
+void nn_set_tensor_cores(NNet &n, int on) { n.tensor_cores = on ? 1 : 0; }
 
 void nn_apply_pyq(NNet &n, const GaugeHandle &G, void *out, const void *in) {
   Context &ctx = context();
@@ -129,6 +148,7 @@ void nn_apply_pyq(NNet &n, const GaugeHandle &G, void *out, const void *in) {
   launch_nn_to_soa64(Vh, n.out.as<float2>(), t.data.p, ctx.stream);
   launch_convert(SOA64, AOS64, Vh, t.data.p, nullptr, out, nullptr, ctx.stream);
   QCU_CUDA(cudaStreamSynchronize(ctx.stream));
+  nn_check(n);
 }
 
 // gradient of L = mean_i |N(r_i) - e_i|^2 / |e_i|^2 over a batch of odd half

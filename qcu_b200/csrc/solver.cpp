@@ -598,6 +598,7 @@ SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParam
     if (prm.solver == 1 && !info.fallback) {
       info.status = ST_RUNNING;
       run_gcr(dP, d64, w, vs, prm, tol2, info);
+      if (prm.precond != 0) nn_check(*prm.nn);
       if ((info.status == ST_STALLED || info.status == ST_BREAKDOWN || info.status == ST_NAN) &&
           info.iterations < prm.maxiter) {
         // the plain solver finishes: FP64 BiCGSTAB from the last FP64 iterate

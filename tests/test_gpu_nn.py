@@ -23,7 +23,31 @@ def _random_weights(seed, scale=0.3):
 
 
 @pytest.mark.parametrize("latt,t_bc", [([4, 4, 4, 8], -1.0), ([6, 4, 2, 4], 1.0)])
-def test_forward_matches_oracle(q, latt, t_bc):
+def test_forward_fma_matches_oracle(q, latt, t_bc):
+    U = O.gauge_haar(latt, 5)
+    r = O.fermion_gauss(O.half_shape(latt), 6)
+    w = _random_weights(7)
+    net = q.Network()
+    net.set_weights(w)
+    net.set_tensor_cores(False)
+    with q.Gauge(dev(U), latt, t_boundary=t_bc) as G:
+        out = empty_like_dev(O.half_shape(latt))
+        net.apply(G, out, dev(r))
+    lat = R.Lattice(U, latt, t_bc)
+    ref, _, _ = R.forward(lat, R.bf16_round(w).astype(np.float64), r.reshape(1, lat.Vh, 4, 3))
+    # the FMA layers: bf16 weights (rounded identically), FP32 links and FP32 arithmetic
+    assert rel(host(out).reshape(ref.shape), ref) < 2e-5
+
+
+@pytest.mark.parametrize("latt,t_bc", [([4, 4, 4, 8], -1.0), ([6, 4, 2, 4], 1.0), ([16, 16, 16, 32], -1.0)])
+def test_forward_tensor_cores_match_oracle(q, latt, t_bc):
+    """The tcgen05 layers (the default for inference): transported inputs
+    rounded to bf16 as the MMA's A operand, bf16 weights, FP32 accumulation.
+    Against the oracle that rounds the same operands: within 1e-3 (a
+    transport computed in FP32 here and in FP64 there can round to the
+    neighbouring bf16 value); against the unrounded network within the bf16
+    resolution.  16^3 x 32 has more 128-site tiles than resident CTAs, so
+    the CTAs loop over tiles; 6x4x2x4 ends in a partial tile."""
     U = O.gauge_haar(latt, 5)
     r = O.fermion_gauss(O.half_shape(latt), 6)
     w = _random_weights(7)
@@ -32,10 +56,16 @@ def test_forward_matches_oracle(q, latt, t_bc):
     with q.Gauge(dev(U), latt, t_boundary=t_bc) as G:
         out = empty_like_dev(O.half_shape(latt))
         net.apply(G, out, dev(r))
+        out2 = empty_like_dev(O.half_shape(latt))
+        net.apply(G, out2, dev(r))
+    got = host(out)
+    assert np.array_equal(got, host(out2))  # deterministic
     lat = R.Lattice(U, latt, t_bc)
-    ref, _, _ = R.forward(lat, R.bf16_round(w).astype(np.float64), r.reshape(1, lat.Vh, 4, 3))
-    # inference uses bf16 weights (rounded identically), FP32 links and FP32 arithmetic
-    assert rel(host(out).reshape(ref.shape), ref) < 2e-5
+    wb = R.bf16_round(w).astype(np.float64)
+    ref, _, _ = R.forward(lat, wb, r.reshape(1, lat.Vh, 4, 3), round_act=True)
+    assert rel(got.reshape(ref.shape), ref) < 1e-3
+    exact, _, _ = R.forward(lat, wb, r.reshape(1, lat.Vh, 4, 3))
+    assert rel(got.reshape(exact.shape), exact) < 1e-2
 
 
 def test_gradient_matches_oracle(q):
