@@ -103,12 +103,16 @@ def layer(lat, W, f, out_parities, round_act=False):
 
 
 def forward(lat, w, r_odd, round_act=False):
-    """N(r) for odd half spinors r [B, Vh, 4, 3] -> (output odd [B, Vh, 4, 3], hidden)"""
+    """N(r) for odd half spinors r [B, Vh, 4, 3] -> (output odd [B, Vh, 4, 3], hidden).
+    round_act: the tensor-core network, whose MMA operands (the transported
+    inputs) are bf16 and whose hidden field is stored as bf16."""
     w1, w2 = split_weights(w)
     B = r_odd.shape[0]
     f0 = np.zeros((B, 2, lat.Vh, C_IN, 3), complex)
     f0[:, 1] = r_odd
     hid = layer(lat, w1, f0, (0, 1), round_act)
+    if round_act:
+        hid = bf16_round_complex(hid)
     out = layer(lat, w2, hid, (1,), round_act)
     return out[:, 1], hid, f0
 

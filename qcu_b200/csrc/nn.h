@@ -35,10 +35,14 @@ struct PtcArgs {
 
 // forward (or adjoint) layer; cin/cout in {4, 16}
 void launch_ptc(int cin, int cout, const Geom &g, const PtcArgs &a, cudaStream_t s);
-// the forward layer with bf16 weights on the tensor cores (nn_tc.cu): the
-// transported inputs are rounded to bf16, accumulation is FP32; err is set
-// to 1 if a wait of the kernel timed out
-void launch_ptc_tc(int cin, int cout, const Geom &g, const PtcArgs &a, int *err, int sms, cudaStream_t s);
+// the network's forward pass with bf16 weights on the tensor cores
+// (nn_tc.cu): z64 = N(r64) on odd-parity FP64 site-blocked spinors (SOA64;
+// z64 may be r64), through a hidden field stored as bf16 pairs
+// (nn_hid16_bytes); the transported inputs are rounded to bf16, accumulation
+// is FP32; err is set to 1 if a wait of the kernel timed out
+void launch_nn_tc(const Geom &g, const void *gauge16, float t_bc, const uint32_t *w16_1, const uint32_t *w16_2,
+                  const void *r64, void *hid16, void *z64, int *err, int sms, cudaStream_t s);
+size_t nn_hid16_bytes(int Vh);
 
 // grad[h][a][b] += sum_x sum_colour delta_a(x) conj((T_h in_b)(x)), over the
 // output parities in a.out_mask (a.out holds delta).  grad: [9][cout][cin] complex FP32.

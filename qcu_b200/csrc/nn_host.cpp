@@ -21,6 +21,7 @@ struct NNet {
   DevBuf w, w16, m, v, grad;       // FP32 master, bf16 copy, Adam moments, gradient
   DevBuf in, hid, out, delta2, delta1, target, enorm, loss;  // work fields (grown to batch x lattice)
   DevBuf err;   // set by the tensor-core layers if a wait timed out
+  DevBuf hid16; // hidden field of the tensor-core layers (bf16 pairs)
   int tensor_cores = 1;
   int step = 0;
   int batch_cap = 0, vh_cap = 0;
@@ -105,10 +106,7 @@ static void forward(NNet &n, const GaugeHandle &G, int B, bool bf16, cudaStream_
   a.out_mask = 3;
   if (bf16) a.w16 = n.w16_1();
   else a.w = n.w1();
-  const bool tc = bf16 && n.tensor_cores;
-  Context &ctx = context();
-  if (tc) launch_ptc_tc(NN_C_IN, NN_C_HID, G.g, a, n.err.as<int>(), ctx.sms, s);
-  else launch_ptc(NN_C_IN, NN_C_HID, G.g, a, s);
+  launch_ptc(NN_C_IN, NN_C_HID, G.g, a, s);
   PtcArgs b2 = a;
   b2.in = n.hid.as<float2>();
   b2.out = n.out.as<float2>();
@@ -118,8 +116,22 @@ static void forward(NNet &n, const GaugeHandle &G, int B, bool bf16, cudaStream_
   b2.w16 = nullptr;
   if (bf16) b2.w16 = n.w16_2();
   else b2.w = n.w2();
-  if (tc) launch_ptc_tc(NN_C_HID, NN_C_OUT, G.g, b2, n.err.as<int>(), ctx.sms, s);
-  else launch_ptc(NN_C_HID, NN_C_OUT, G.g, b2, s);
+  launch_ptc(NN_C_HID, NN_C_OUT, G.g, b2, s);
+}
+
+// z = N(r) on odd-parity SOA64 spinors (z may be r): the tensor-core layers,
+// or the FMA layers through the NN layout
+static void apply_soa64(NNet &n, const GaugeHandle &G, const void *r64, void *z64, cudaStream_t s) {
+  const int Vh = G.g.Vh;
+  if (n.tensor_cores) {
+    n.hid16.ensure(nn_hid16_bytes(Vh));
+    launch_nn_tc(G.g, G.g16.p, (float)G.t_bc, n.w16_1(), n.w16_2(), r64, n.hid16.p, z64, n.err.as<int>(),
+                 context().sms, s);
+    return;
+  }
+  launch_soa64_to_nn(Vh, r64, n.in.as<float2>(), s);
+  forward(n, G, 1, true, s);
+  launch_nn_to_soa64(Vh, n.out.as<float2>(), z64, s);
 }
 
 void nn_check(NNet &n) {
@@ -137,15 +149,13 @@ void nn_apply_pyq(NNet &n, const GaugeHandle &G, void *out, const void *in) {
   Context &ctx = context();
   std::lock_guard<std::mutex> lk(ctx.mu);
   const int Vh = G.g.Vh;
-  n.ensure(1, Vh);
+  if (!n.tensor_cores) n.ensure(1, Vh);  // the FMA layers' work fields
   QCU_CUDA(cudaDeviceSynchronize());
-  // complex128 -> complex64 odd slab, via the FP64 blocked layout
+  // complex128 -> FP64 blocked layout, the network, and back
   Spinor &t = stage();
   t.alloc(SOA64, Vh);
   launch_convert(AOS64, SOA64, Vh, in, nullptr, t.data.p, nullptr, ctx.stream);
-  launch_soa64_to_nn(Vh, t.data.p, n.in.as<float2>(), ctx.stream);
-  forward(n, G, 1, true, ctx.stream);
-  launch_nn_to_soa64(Vh, n.out.as<float2>(), t.data.p, ctx.stream);
+  apply_soa64(n, G, t.data.p, t.data.p, ctx.stream);
   launch_convert(SOA64, AOS64, Vh, t.data.p, nullptr, out, nullptr, ctx.stream);
   QCU_CUDA(cudaStreamSynchronize(ctx.stream));
   nn_check(n);
@@ -226,12 +236,12 @@ double nn_train_step(NNet &n, const GaugeHandle &G, const void *r, const void *e
 
 // GCR preconditioner application on FP64 blocked odd spinors: z = N(r)
 void nn_apply_soa64(NNet &n, const GaugeHandle &G, const void *r64, void *z64, cudaStream_t s) {
-  const int Vh = G.g.Vh;
-  launch_soa64_to_nn(Vh, r64, n.in.as<float2>(), s);
-  forward(n, G, 1, true, s);
-  launch_nn_to_soa64(Vh, n.out.as<float2>(), z64, s);
+  apply_soa64(n, G, r64, z64, s);
 }
 
-void nn_prepare(NNet &n, int Vh) { n.ensure(1, Vh); }
+void nn_prepare(NNet &n, int Vh) {
+  if (n.tensor_cores) n.hid16.ensure(nn_hid16_bytes(Vh));
+  else n.ensure(1, Vh);
+}
 
 }  // namespace qcu

@@ -5,6 +5,7 @@
     python -m qcu_b200.perf batch  --csw 1.0 --kappa 0.128
     python -m qcu_b200.perf precisions
     python -m qcu_b200.perf legacy --iters 20
+    python -m qcu_b200.perf nn --iters 20
 
 `dslash` applies the even-odd hopping term `iters` times (after 3 warm-up
 launches) on a seeded smooth gauge field and prints the time per launch and
@@ -17,7 +18,10 @@ main lattice together with 4 Gaussian right-hand sides on each of
 prints the batched wall time next to the same 24 systems solved one at a
 time.  `legacy` calls dslashQcu (qcu's ABI: PyQuda-layout complex128
 fields, one kernel per call) `iters` times and prints the wall time per
-synchronous call.  `precisions` solves one system (default: the benchmark's) with plain
+synchronous call.  `nn` applies the learned preconditioner's network
+(random weights, scale 0.3) `iters` times on an odd half spinor and prints
+the time per application with the tensor-core layers and with the FP32 FMA
+layers.  `precisions` solves one system (default: the benchmark's) with plain
 FP64 BiCGSTAB, BiCGSTAB with FP64 reliable updates at 32 and 16 bits, and
 the FP64 GCR around 32- and 16-bit inner solves, and states each solution's
 difference from the FP64 one.  Inputs are
@@ -48,7 +52,7 @@ def _gauge(latt, eps, seed, t_bc, csw=0.0, kappa=0.0):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["dslash", "solve", "batch", "precisions", "legacy"])
+    ap.add_argument("what", choices=["dslash", "solve", "batch", "precisions", "legacy", "nn"])
     ap.add_argument("--latt", type=int, nargs=4, default=[32, 32, 32, 64])
     ap.add_argument("--eps", type=float, default=0.25)
     ap.add_argument("--seed", type=int, default=20251203)
@@ -85,6 +89,34 @@ def main(argv=None):
         return
     if a.what == "batch":
         _batch(a)
+        return
+    if a.what == "nn":
+        import numpy as np
+
+        G, u, L = _gauge(a.latt, a.eps, a.seed, a.t_bc, a.csw, a.kappa)
+        del u
+        r = torch.empty(L.half, dtype=torch.complex128, device="cuda")
+        q.fermion_random(r, r.numel(), 0, 7)
+        out = torch.empty_like(r)
+        net = q.Network(seed=1)
+        w = np.random.default_rng(3).normal(0, 0.3, q.Network.num_params()).astype(np.float32)
+        net.set_weights(w)
+        stream = torch.cuda.ExternalStream(q.stream_handle())
+        res = {"kernel": "nn", "latt": a.latt}
+        for name, on in (("tensor_cores", True), ("fma", False)):
+            net.set_tensor_cores(on)
+            for _ in range(2):
+                net.apply(G, out, r)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(a.iters):
+                net.apply(G, out, r)
+            e1.record(stream)
+            e1.synchronize()
+            res[name + "_ms_per_apply"] = round(e0.elapsed_time(e1) / a.iters, 4)
+        print(json.dumps(res))
+        net.close()
+        G.close()
         return
     if a.what == "legacy":
         L = q.Layout(tuple(a.latt))

@@ -42,11 +42,13 @@ def test_forward_fma_matches_oracle(q, latt, t_bc):
 @pytest.mark.parametrize("latt,t_bc", [([4, 4, 4, 8], -1.0), ([6, 4, 2, 4], 1.0), ([16, 16, 16, 32], -1.0)])
 def test_forward_tensor_cores_match_oracle(q, latt, t_bc):
     """The tcgen05 layers (the default for inference): transported inputs
-    rounded to bf16 as the MMA's A operand, bf16 weights, FP32 accumulation.
-    Against the oracle that rounds the same operands: within 1e-3 (a
-    transport computed in FP32 here and in FP64 there can round to the
-    neighbouring bf16 value); against the unrounded network within the bf16
-    resolution.  16^3 x 32 has more 128-site tiles than resident CTAs, so
+    rounded to bf16 as the MMA's A operand, bf16 weights, FP32 accumulation,
+    the hidden field stored as bf16, 16-bit links.  Against the oracle that
+    rounds the same operands: within 3e-3 (a value computed in FP32 from
+    16-bit links here and in FP64 there can round to the neighbouring bf16
+    value, one unit of 2^-8 relative, at each of the two roundings: the
+    stored hidden field and the transported operand); against the unrounded
+    network within the bf16 resolution.  16^3 x 32 has more 128-site tiles than resident CTAs, so
     the CTAs loop over tiles; 6x4x2x4 ends in a partial tile."""
     U = O.gauge_haar(latt, 5)
     r = O.fermion_gauss(O.half_shape(latt), 6)
@@ -63,7 +65,7 @@ def test_forward_tensor_cores_match_oracle(q, latt, t_bc):
     lat = R.Lattice(U, latt, t_bc)
     wb = R.bf16_round(w).astype(np.float64)
     ref, _, _ = R.forward(lat, wb, r.reshape(1, lat.Vh, 4, 3), round_act=True)
-    assert rel(got.reshape(ref.shape), ref) < 1e-3
+    assert rel(got.reshape(ref.shape), ref) < 3e-3
     exact, _, _ = R.forward(lat, wb, r.reshape(1, lat.Vh, 4, 3))
     assert rel(got.reshape(exact.shape), exact) < 1e-2
 
