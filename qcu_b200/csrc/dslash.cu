@@ -38,8 +38,9 @@ namespace qcu {
 // 16-bit kernels and slower for the FP32 ones.
 #define DSLASH_SPLIT_RED(K) ((K) == SOA16)
 #define DSLASH_RED_BLOCKS(K) ((K) == SOA16 ? QCU_DSLASH16_RED_BLOCKS : 3)
-#define DSLASH_MIN_BLOCKS(K, RED) \
-  (((K) == AOS64 || (K) == SOA64) ? 3 : ((RED) == RED_NONE ? QCU_DSLASH32_BLOCKS : DSLASH_RED_BLOCKS(K)))
+#define DSLASH_MIN_BLOCKS(K, RED)                     \
+  (((K) == AOS64 || (K) == AOS64W || (K) == SOA64) ? 3 \
+                                                   : ((RED) == RED_NONE ? QCU_DSLASH32_BLOCKS : DSLASH_RED_BLOCKS(K)))
 
 // FP32 and 16-bit spinors: the hop and the epilogue on spin-paired registers
 // in FP32 arithmetic (hop32.cuh)
@@ -235,7 +236,12 @@ static void launch_clov(const Geom &g, const DslashArgs &a, Context &ctx, cudaSt
 
 void launch_dslash(int kind, int gkind, int ckind, const Geom &g, const DslashArgs &a, Context &ctx,
                    cudaStream_t s) {
-  if (kind == AOS64 && gkind == GAOS64 && ckind == CSOA64) launch_clov<AOS64, GAOS64, CSOA64>(g, a, ctx, s);
+  // PyQuda-layout spinors whose buffers are all 32-byte aligned take the 32-byte accesses
+  auto al32 = [](const void *p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 31) == 0; };
+  if (kind == AOS64 && gkind == GAOS64 && ckind == CSOA64 && al32(a.in) && al32(a.out) && al32(a.x1) &&
+      al32(a.x2) && al32(a.rt))
+    launch_clov<AOS64W, GAOS64, CSOA64>(g, a, ctx, s);
+  else if (kind == AOS64 && gkind == GAOS64 && ckind == CSOA64) launch_clov<AOS64, GAOS64, CSOA64>(g, a, ctx, s);
   else if (kind == SOA64 && gkind == GSOA64 && ckind == CSOA64) launch_clov<SOA64, GSOA64, CSOA64>(g, a, ctx, s);
   else if (kind == SOA32 && gkind == GSOA32 && ckind == CSOA32) launch_clov<SOA32, GSOA32, CSOA32>(g, a, ctx, s);
   else if (kind == SOA16 && gkind == GSOA16 && ckind == CSOA32) launch_clov<SOA16, GSOA16, CSOA32>(g, a, ctx, s);

@@ -12,6 +12,8 @@
 //   AOS64 : PyQuda's own layout, complex128 [site][spin*3+colour]
 //           (python/PyQuda/pyquda/field.py:78,230) -- used by the legacy ABI
 //           so a single dslash needs no layout conversion at all.
+//   AOS64W: the same layout, read and written with 32-byte accesses; for
+//           fields whose base is 32-byte aligned (the legacy dslash checks)
 //   SOA64 : double2, NC = 12 (one complex per 16-byte load)
 //   SOA32 : float4,  NC = 6: float4 j = 3 * q + c holds colour c of spins 2q
 //           and 2q + 1 as (re, re, im, im), the lane pairs of the paired FP32
@@ -35,12 +37,13 @@
 
 namespace qcu {
 
-enum SpinorKind { AOS64 = 0, SOA64 = 1, SOA32 = 2, SOA16 = 3 };
+enum SpinorKind { AOS64 = 0, SOA64 = 1, SOA32 = 2, SOA16 = 3, AOS64W = 4 };
 enum GaugeKind { GAOS64 = 0, GSOA64 = 1, GSOA32 = 2, GSOA16 = 3 };
 
 template <int K> struct SpinorReal { using T = float; };
 template <> struct SpinorReal<AOS64> { using T = double; };
 template <> struct SpinorReal<SOA64> { using T = double; };
+template <> struct SpinorReal<AOS64W> { using T = double; };
 
 // 16-bit fixed point: two values per 32-bit word, each stored offset-binary
 // (u = v + 32768, v = round(x * 32767) in [-32767, 32767]).
@@ -151,6 +154,18 @@ __device__ __forceinline__ void spinor_load(const SpinorView<K> &v, int s, Cpx<T
       double2 d = __ldg(p + c);
       out[c] = Cpx<T>((T)d.x, (T)d.y);
     }
+  } else if constexpr (K == AOS64W) {
+    // 32-byte loads (two complex numbers each) of a 32-byte aligned field: a
+    // warp's request over 32 site-major records costs as many L1 wavefronts
+    // as a 16-byte one, for twice the data
+    const double2 *p = static_cast<const double2 *>(v.p) + (size_t)s * 12;
+#pragma unroll
+    for (int c = 0; c < 12; c += 2) {
+      unsigned w[8];
+      ldg256(p + c, w);
+      out[c] = Cpx<T>((T)__hiloint2double(w[1], w[0]), (T)__hiloint2double(w[3], w[2]));
+      out[c + 1] = Cpx<T>((T)__hiloint2double(w[5], w[4]), (T)__hiloint2double(w[7], w[6]));
+    }
   } else if constexpr (K == SOA64) {
     const double2 *p = static_cast<const double2 *>(v.p) + blk_base<12>(s);
 #pragma unroll
@@ -192,6 +207,19 @@ __device__ __forceinline__ void spinor_store(const SpinorView<K> &v, int s, cons
     double2 *p = static_cast<double2 *>(v.p) + (size_t)s * 12;
 #pragma unroll
     for (int c = 0; c < 12; c++) p[c] = make_double2((double)in[c].re, (double)in[c].im);
+  } else if constexpr (K == AOS64W) {
+    double2 *p = static_cast<double2 *>(v.p) + (size_t)s * 12;
+#pragma unroll
+    for (int c = 0; c < 12; c += 2) {
+      const double v4[4] = {(double)in[c].re, (double)in[c].im, (double)in[c + 1].re, (double)in[c + 1].im};
+      unsigned w[8];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        w[2 * k] = (unsigned)__double2loint(v4[k]);
+        w[2 * k + 1] = (unsigned)__double2hiint(v4[k]);
+      }
+      stg256(p + c, w);
+    }
   } else if constexpr (K == SOA64) {
     double2 *p = static_cast<double2 *>(v.p) + blk_base<12>(s);
 #pragma unroll

@@ -384,3 +384,25 @@ def test_dslashQcu_on_pyquda_weak_field_lime(q):
     assert res["status"] == 1
     r = psi - O.mfull(host(x), U, latt, kappa, -1.0, True, A[0], A[1])
     assert np.linalg.norm(r) / np.linalg.norm(psi) <= 1.05e-10
+
+
+def test_dslashQcu_16_byte_aligned_buffers(q):
+    """dslashQcu reads 32-byte aligned PyQuda buffers with 32-byte accesses;
+    buffers that are only 16-byte aligned (a complex128 view one element into
+    an allocation) take the 16-byte path and give the same result."""
+    import torch
+
+    latt = [8, 4, 4, 8]
+    U, psi = _fields(latt, "haar", 21)
+    ref = O.dslash(psi[0], U, latt, 1)
+    n = int(np.prod(O.half_shape(latt)))
+    for shift in (0, 1):  # elements of 16 bytes
+        src = torch.zeros(n + 1, dtype=torch.complex128, device="cuda")
+        src[shift:shift + n] = torch.from_numpy(np.ascontiguousarray(psi[0]).reshape(-1)).cuda()
+        dst = torch.full((n + 1,), float("nan"), dtype=torch.complex128, device="cuda")
+        pin, pout = src[shift:shift + n], dst[shift:shift + n]
+        assert (pin.data_ptr() % 32 == 0) == (shift == 0)
+        q.dslashQcu(pout, pin, dev(U), q.QcuParam(latt), 1)
+        assert q.last_error()[0] == 0
+        assert rel(host(pout).reshape(ref.shape), ref) <= 1e-13
+        assert np.isnan(host(dst)[shift + n:]).all() and np.isnan(host(dst)[:shift]).all()
