@@ -233,6 +233,49 @@ int qcuNNSetTensorCores(qcuNN net, int on);
 int qcuNNTrainStep(qcuNN net, qcuGauge h, const void *r, const void *e, int batch, double lr, double *loss,
                    float *grad);
 
+/* Two-level adaptive aggregation multigrid for the full operator
+ * M = A - kappa D (Wilson, or clover when the handle has a clover term).
+ * No counterpart in qcu, whose src/multgrid.cu is empty; the parameters are
+ * those PyQuda passes to QUDA's multigrid (python/PyQuda/pyquda/dslash/
+ * general.py:121-230), the defaults its Wilson and clover dslash classes use
+ * (dslash/wilson.py:24) with two levels and fewer near-null vectors.
+ * Set-up: n_vec near-null vectors (each the error left by setup_maxiter
+ * iterations of FP32 BiCGSTAB on M y = M v0, v0 Gaussian), orthonormalised
+ * on every aggregate of geo_block_size sites and chirality, and the Galerkin
+ * coarse operator P^dag M P (2 n_vec complex degrees of freedom per
+ * aggregate).  Solve: FP64 flexible GCR(gcr_k) on the full system, each step
+ * preconditioned by nu_pre MR steps, the coarse correction (FP32 BiCGSTAB to
+ * coarse_tol, at most coarse_maxiter iterations) and nu_post MR steps. */
+typedef struct qcuMG_s *qcuMG;
+typedef struct {
+  int geo_block_size[4]; /* aggregate extents x (full), y, z, t; the x extent even, the
+                            product a multiple of 32 and at most 512, each dividing the lattice */
+  int n_vec;             /* near-null vectors, 1..16 */
+  int setup_maxiter;
+  double coarse_tol;
+  int coarse_maxiter;
+  int nu_pre;
+  int nu_post;
+  int gcr_k;             /* outer GCR directions kept before a restart, 1..32 */
+} qcuMGParam;
+typedef struct {
+  int outer;             /* outer GCR steps (one two-level cycle each) */
+  int coarse_iters;      /* coarse BiCGSTAB iterations, summed */
+  int status;            /* 1 converged, 2 max outer steps, 3 breakdown, 4 NaN/Inf */
+  double true_residual;  /* ||b - M x|| / ||b||, FP64 */
+  double seconds;
+} qcuMGResult;
+void qcuMGParamDefault(qcuMGParam *p);
+/* the gauge handle must outlive the multigrid; set-up runs on the current device */
+int qcuMGCreate(qcuMG *mg, qcuGauge h, double kappa, const qcuMGParam *p, double *setup_seconds);
+int qcuMGFree(qcuMG mg);
+/* x, b: full spinors (PyQuda layout, complex128, device); x starts from zero;
+ * stops at ||b - M x|| <= tol ||b|| or maxiter outer steps */
+int qcuMGInvert(qcuMG mg, void *x, const void *b, double tol, int maxiter, qcuMGResult *r);
+/* set-up checks on a seeded coarse vector c: |P^dag P c - c| / |c| and
+ * |A_c c - P^dag M P c| / |P^dag M P c| */
+int qcuMGCheck(qcuMG mg, double *orth_err, double *galerkin_err);
+
 /* number of kernels this library has launched in this process (graph
  * replays count every node) */
 long long qcuKernelLaunches(void);

@@ -109,6 +109,32 @@ class QcuBatchSystem(ctypes.Structure):
     ]
 
 
+class QcuMGParam(ctypes.Structure):
+    _fields_ = [
+        ("geo_block_size", ctypes.c_int * 4),
+        ("n_vec", ctypes.c_int),
+        ("setup_maxiter", ctypes.c_int),
+        ("coarse_tol", ctypes.c_double),
+        ("coarse_maxiter", ctypes.c_int),
+        ("nu_pre", ctypes.c_int),
+        ("nu_post", ctypes.c_int),
+        ("gcr_k", ctypes.c_int),
+    ]
+
+
+class QcuMGResult(ctypes.Structure):
+    _fields_ = [
+        ("outer", ctypes.c_int),
+        ("coarse_iters", ctypes.c_int),
+        ("status", ctypes.c_int),
+        ("true_residual", ctypes.c_double),
+        ("seconds", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class QcuBatchTune(ctypes.Structure):
     _fields_ = [("dslash_threads", ctypes.c_int), ("dslash_rhs", ctypes.c_int), ("blas_sites", ctypes.c_int),
                 ("mma", ctypes.c_int)]
@@ -164,6 +190,13 @@ _lib.qcuNNApply.argtypes = [_vp, _vp, _vp, _vp]
 _lib.qcuNNSetTensorCores.argtypes = [_vp, ctypes.c_int]
 _lib.qcuNNTrainStep.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
                                 ctypes.c_void_p]
+_lib.qcuMGParamDefault.argtypes = [ctypes.POINTER(QcuMGParam)]
+_lib.qcuMGParamDefault.restype = None
+_lib.qcuMGCreate.argtypes = [ctypes.POINTER(_vp), _vp, ctypes.c_double, ctypes.POINTER(QcuMGParam),
+                             ctypes.POINTER(ctypes.c_double)]
+_lib.qcuMGFree.argtypes = [_vp]
+_lib.qcuMGInvert.argtypes = [_vp, _vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(QcuMGResult)]
+_lib.qcuMGCheck.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
 _lib.qcuBenchDslash.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_double)]
 
@@ -575,6 +608,54 @@ class Network:
     def close(self):
         if self._h:
             _lib.qcuNNFree(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Multigrid:
+    """Two-level adaptive aggregation multigrid (qcuMG) for the full operator
+    M = A - kappa D of a Gauge; parameters as PyQuda's multigrid set-up
+    (geo_block_size, n_vec, setup_maxiter, coarse_tol, coarse_maxiter,
+    nu_pre, nu_post) plus gcr_k, the outer GCR restart length.  The gauge
+    must stay open while the multigrid is used."""
+
+    def __init__(self, gauge: "Gauge", kappa: float, **params):
+        p = QcuMGParam()
+        _lib.qcuMGParamDefault(ctypes.byref(p))
+        for k, v in params.items():
+            if k == "geo_block_size":
+                p.geo_block_size = (ctypes.c_int * 4)(*[int(x) for x in v])
+            elif k in dict(QcuMGParam._fields_):
+                setattr(p, k, v)
+            else:
+                raise TypeError(f"unknown multigrid parameter {k!r}")
+        self.gauge = gauge
+        self.kappa = kappa
+        self._h = _vp()
+        secs = ctypes.c_double(0)
+        _check(_lib.qcuMGCreate(ctypes.byref(self._h), gauge._h, float(kappa), ctypes.byref(p), ctypes.byref(secs)))
+        self.setup_seconds = secs.value
+
+    def invert(self, x, b, tol: float = 1e-10, maxiter: int = 1000) -> dict:
+        """x = M^-1 b on full PyQuda-layout spinors (complex128, device)."""
+        r = QcuMGResult()
+        _check(_lib.qcuMGInvert(self._h, _ptr(x), _ptr(b), float(tol), int(maxiter), ctypes.byref(r)))
+        return r.as_dict()
+
+    def check(self):
+        """(|P^dag P c - c| / |c|, |A_c c - P^dag M P c| / |P^dag M P c|) for a seeded coarse c."""
+        o, g = ctypes.c_double(0), ctypes.c_double(0)
+        _check(_lib.qcuMGCheck(self._h, ctypes.byref(o), ctypes.byref(g)))
+        return o.value, g.value
+
+    def close(self):
+        if self._h:
+            _lib.qcuMGFree(self._h)
             self._h = _vp()
 
     def __del__(self):

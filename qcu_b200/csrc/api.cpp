@@ -4,6 +4,7 @@
 
 #include "batch.h"
 #include "dd.h"
+#include "mg.h"
 #include "nn.h"
 #include "solver.h"
 
@@ -26,6 +27,9 @@ struct qcuGauge_s {
 };
 struct qcuNN_s {
   NNet *n;
+};
+struct qcuMG_s {
+  MG *m;
 };
 
 #define QCU_API_BEGIN \
@@ -436,6 +440,69 @@ int qcuNNTrainStep(qcuNN net, qcuGauge h, const void *r, const void *e, int batc
   require(net && h && r && e && batch > 0, "bad arguments");
   const double l = nn_train_step(*net->n, *h->h, r, e, batch, lr, grad);
   if (loss) *loss = l;
+  QCU_API_END
+}
+
+void qcuMGParamDefault(qcuMGParam *p) {
+  if (!p) return;
+  const MGParams d;
+  for (int k = 0; k < 4; k++) p->geo_block_size[k] = d.geo_block_size[k];
+  p->n_vec = d.n_vec;
+  p->setup_maxiter = d.setup_maxiter;
+  p->coarse_tol = d.coarse_tol;
+  p->coarse_maxiter = d.coarse_maxiter;
+  p->nu_pre = d.nu_pre;
+  p->nu_post = d.nu_post;
+  p->gcr_k = d.gcr_k;
+}
+
+int qcuMGCreate(qcuMG *mg, qcuGauge h, double kappa, const qcuMGParam *p, double *setup_seconds) {
+  QCU_API_BEGIN
+  require(mg != nullptr && h != nullptr, "null argument");
+  MGParams q;
+  if (p) {
+    for (int k = 0; k < 4; k++) q.geo_block_size[k] = p->geo_block_size[k];
+    q.n_vec = p->n_vec;
+    q.setup_maxiter = p->setup_maxiter;
+    q.coarse_tol = p->coarse_tol;
+    q.coarse_maxiter = p->coarse_maxiter;
+    q.nu_pre = p->nu_pre;
+    q.nu_post = p->nu_post;
+    q.gcr_k = p->gcr_k;
+  }
+  MG *m = mg_create(*h->h, kappa, q);
+  if (setup_seconds) *setup_seconds = mg_setup_seconds(*m);
+  *mg = new qcuMG_s{m};
+  QCU_API_END
+}
+
+int qcuMGFree(qcuMG mg) {
+  QCU_API_BEGIN
+  if (mg) {
+    mg_free(mg->m);
+    delete mg;
+  }
+  QCU_API_END
+}
+
+int qcuMGInvert(qcuMG mg, void *x, const void *b, double tol, int maxiter, qcuMGResult *r) {
+  QCU_API_BEGIN
+  require(mg != nullptr, "null multigrid");
+  const MGInfo i = mg_solve(*mg->m, x, b, tol, maxiter);
+  if (r) {
+    r->outer = i.outer;
+    r->coarse_iters = i.coarse_iters;
+    r->status = i.status;
+    r->true_residual = i.true_residual;
+    r->seconds = i.seconds;
+  }
+  QCU_API_END
+}
+
+int qcuMGCheck(qcuMG mg, double *orth_err, double *galerkin_err) {
+  QCU_API_BEGIN
+  require(mg && orth_err && galerkin_err, "null argument");
+  mg_check(*mg->m, orth_err, galerkin_err);
   QCU_API_END
 }
 
