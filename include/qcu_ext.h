@@ -24,6 +24,7 @@ extern "C" {
 
 typedef struct qcuGauge_s *qcuGauge;
 typedef struct qcuNN_s *qcuNN;  /* learned preconditioner (see qcuNNCreate) */
+typedef struct qcuMG_s *qcuMG;  /* two-level multigrid (see qcuMGCreate) */
 
 /* last error of the calling thread: returns its code, copies the message */
 int qcuGetLastError(char *msg, int len);
@@ -68,8 +69,11 @@ typedef struct {
   int gauge_precision;   /* 0: links stored like the spinors; 16 (with precision 32): FP32
                             spinors and 16-bit links in the inner operator */
   int precond;           /* GCR preconditioner: 0 inner BiCGSTAB; 1 the network `nn`;
-                            2 the network, then the inner BiCGSTAB on what it leaves */
+                            2 the network, then the inner BiCGSTAB on what it leaves;
+                            3 the multigrid `mg`'s coarse-grid correction, then the inner
+                            BiCGSTAB on what it leaves (mg built on this handle and kappa) */
   qcuNN nn;
+  qcuMG mg;
 } qcuInvertParam;
 
 typedef struct {
@@ -246,7 +250,6 @@ int qcuNNTrainStep(qcuNN net, qcuGauge h, const void *r, const void *e, int batc
  * aggregate).  Solve: FP64 flexible GCR(gcr_k) on the full system, each step
  * preconditioned by nu_pre MR steps, the coarse correction (FP32 BiCGSTAB to
  * coarse_tol, at most coarse_maxiter iterations) and nu_post MR steps. */
-typedef struct qcuMG_s *qcuMG;
 typedef struct {
   int geo_block_size[4]; /* aggregate extents x (full), y, z, t; the x extent even, the
                             product a multiple of 32 and at most 512, each dividing the lattice */

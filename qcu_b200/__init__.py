@@ -79,6 +79,7 @@ class QcuInvertParam(ctypes.Structure):
         ("gauge_precision", ctypes.c_int),
         ("precond", ctypes.c_int),
         ("nn", ctypes.c_void_p),
+        ("mg", ctypes.c_void_p),
     ]
 
 
@@ -325,11 +326,15 @@ class Gauge:
     def invert(self, x, b, kappa: float, tol: float = 1e-10, maxiter: int = 10000, precision: int = 64,
                delta: float = 0.1, clover: bool = False, x0_mode: int = 0, x0_seed: int = 0, abs_tol: bool = False,
                chunk: int = 0, solver: str = "bicgstab", inner_iters: int = 16, inner_tol: float = 0.1,
-               gcr_k: int = 8, gauge_precision: int = 0, precond: int = 0, nn: "Network" = None) -> dict:
+               gcr_k: int = 8, gauge_precision: int = 0, precond: int = 0, nn: "Network" = None,
+               mg: "Multigrid" = None) -> dict:
         """Solve M x = b (full spinors).  solver="bicgstab": BiCGSTAB in
         `precision` with FP64 reliable updates; solver="gcr": FP64 flexible
         GCR(gcr_k) preconditioned by `inner_iters` BiCGSTAB iterations in
-        `precision` (or until the inner residual drops by inner_tol)."""
+        `precision` (or until the inner residual drops by inner_tol).
+        precond: 1 the network nn, 2 nn then the inner solve, 3 the coarse-grid
+        correction of the Multigrid mg (built on this gauge and kappa) then the
+        inner solve."""
         p = QcuInvertParam()
         _lib.qcuInvertParamDefault(ctypes.byref(p))
         p.kappa, p.tol, p.maxiter, p.precision, p.delta = kappa, tol, maxiter, precision, delta
@@ -339,6 +344,7 @@ class Gauge:
         p.gauge_precision = gauge_precision
         p.precond = precond
         p.nn = nn._h.value if nn is not None else None
+        p.mg = mg._h.value if mg is not None else None
         r = QcuInvertResult()
         _check(_lib.qcuInvert(self._h, _ptr(x), _ptr(b), ctypes.byref(p), ctypes.byref(r)))
         return r.as_dict()

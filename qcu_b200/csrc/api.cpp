@@ -194,6 +194,7 @@ void qcuInvertParamDefault(qcuInvertParam *p) {
   p->gauge_precision = d.gauge_precision;
   p->precond = d.precond;
   p->nn = nullptr;
+  p->mg = nullptr;
 }
 
 static SolveParams solve_params(const qcuInvertParam *p) {
@@ -215,6 +216,7 @@ static SolveParams solve_params(const qcuInvertParam *p) {
   s.gauge_precision = p->gauge_precision;
   s.precond = p->precond;
   s.nn = p->nn ? p->nn->n : nullptr;
+  s.mg = p->mg ? p->mg->m : nullptr;
   require(s.tol > 0, "tol must be positive");
   require(s.delta >= 0 && s.delta < 1, "delta must be in [0, 1)");
   return s;

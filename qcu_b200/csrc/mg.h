@@ -38,4 +38,19 @@ MGInfo mg_solve(MG &mg, void *x, const void *b, double tol, int maxiter);
 void mg_check(MG &mg, double *orth_err, double *galerkin_err);
 double mg_setup_seconds(const MG &mg);
 
+// The coarse-grid correction as a preconditioner of the even-odd system
+// M_pc x_o = b_o (solve()'s precond 3): z_o = the odd part of P A_c^-1 P^dag
+// applied to (0, A_o r_o), i.e. A_c's approximation of M_pc^-1 r_o (S^-1 of
+// the Schur complement S = A_o - kappa^2 D_oe A_e^-1 D_eo, M_pc = A_o^-1 S).
+// r_odd, z_odd: FP64 site-blocked half spinors (SOA64); queued on ctx's
+// stream, the caller holds ctx.mu.
+void mg_coarse_odd(MG &mg, Context &ctx, const void *r_odd, void *z_odd);
+// with q = M_pc z on entry: alpha = <q, r> / |q|^2 (the minimal-residual
+// multiple of the correction), z *= alpha, q = r - alpha q; returns alpha
+double2 mg_minres_scale(MG &mg, Context &ctx, void *z, void *q, const void *r);
+// throws unless mg was built on G for this kappa, with the clover term iff G has one
+void mg_require_compatible(const MG &mg, const GaugeHandle &G, double kappa, int use_clover);
+// kernels the coarse solves launched since the last call (read from the device)
+long long mg_take_launches(MG &mg, Context &ctx);
+
 }  // namespace qcu

@@ -15,6 +15,7 @@
 #include "gcr.h"
 #include "nn.h"
 #include "solver.h"
+#include "mg.h"
 
 namespace qcu {
 
@@ -362,13 +363,16 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
   *ctx.st_host = init;
   QCU_CUDA(cudaMemcpyAsync(ctx.st, ctx.st_host, sizeof(SolverState), cudaMemcpyHostToDevice, st));
   // preconditioner: 0 inner solve z = BiCGSTAB(r); 1 z = N(r) (network);
-  // 2 z = N(r) + BiCGSTAB(r - M_pc N(r)).  The inner solve reads `rin`.
+  // 2 z = N(r) + BiCGSTAB(r - M_pc N(r)); 3 the same with N the multigrid's
+  // coarse-grid correction.  The inner solve reads `rin`.
   const int pc = prm.precond;
-  require(pc >= 0 && pc <= 2, "solve: precond must be 0, 1 or 2");
-  require(pc == 0 || prm.nn != nullptr, "solve: the network preconditioner needs a network");
-  if (pc != 0) nn_prepare(*prm.nn, Vh);
+  require(pc >= 0 && pc <= 3, "solve: precond must be 0, 1, 2 or 3");
+  require(pc == 0 || pc == 3 || prm.nn != nullptr, "solve: the network preconditioner needs a network");
+  require(pc != 3 || prm.mg != nullptr, "solve: precond 3 needs a multigrid");
+  if (pc == 1 || pc == 2) nn_prepare(*prm.nn, Vh);
+  if (pc == 3) mg_require_compatible(*prm.mg, dP.G, kappa, prm.use_clover);
   VecSet vin = vs;
-  vin.r64 = pc == 2 ? w.aux.data.p : w.r64.data.p;
+  vin.r64 = pc >= 2 ? w.aux.data.p : w.r64.data.p;
   long long nodes = 0;  // 0: device-side WHILE loop (launches counted from the iteration count)
   long long per_iter = 8;  // kernels per pass of the WHILE body (measured at capture)
   cudaGraphExec_t inner = nullptr;
@@ -424,16 +428,21 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
       }
       best = cycle == 0 ? rr : std::min(best, rr);
       for (int k = 0; k < m && rr > tol2 && info.iterations < prm.maxiter; k++) {
-        if (pc != 0) nn_apply_soa64(*prm.nn, dP.G, w.r64.data.p, gs.znew.data.p, st);
-        if (pc == 2) {  // what the network leaves: aux = r - M_pc N(r)
+        if (pc == 1 || pc == 2) nn_apply_soa64(*prm.nn, dP.G, w.r64.data.p, gs.znew.data.p, st);
+        if (pc == 3) mg_coarse_odd(*prm.mg, ctx, w.r64.data.p, gs.znew.data.p);
+        if (pc == 2) {  // what the first stage leaves: aux = r - M_pc z
           d64(0, gs.znew, w.tmp64, clov, 1.0);
           d64(1, w.tmp64, w.aux, clov, k2, &w.r64, 1.0, &gs.znew, -1.0);
+        } else if (pc == 3) {  // the same after the minimal-residual multiple: aux = M_pc z, then r - alpha aux
+          d64(0, gs.znew, w.tmp64, clov, 1.0);
+          d64(1, w.tmp64, w.aux, clov, -k2, &gs.znew, 1.0);
+          mg_minres_scale(*prm.mg, ctx, gs.znew.data.p, w.aux.data.p, w.r64.data.p);
         }
         if (pc != 1) {
           QCU_CUDA(cudaGraphLaunch(inner, st));
           if (nodes) note_launch(nodes);
         }
-        if (pc == 2) launch_axpby(SOA64, Vh, 1.0, gs.zin.data.p, nullptr, 1.0, gs.znew.data.p, nullptr, st);
+        if (pc >= 2) launch_axpby(SOA64, Vh, 1.0, gs.zin.data.p, nullptr, 1.0, gs.znew.data.p, nullptr, st);
         Spinor &zk = pc == 0 ? gs.zin : gs.znew;
         // w = M_pc z
         d64(0, zk, w.tmp64, clov, 1.0);
@@ -477,6 +486,7 @@ static void run_gcr(Dsl &dP, Dsl &d64, Workspace &w, const VecSet &vs, const Sol
     throw;
   }
   if (inner) cudaGraphExecDestroy(inner);
+  if (pc == 3) note_launch(mg_take_launches(*prm.mg, ctx));
   if (info.status == ST_RUNNING && info.iterations >= prm.maxiter) info.status = ST_MAXITER;
 }
 
@@ -598,7 +608,7 @@ SolveInfo solve(GaugeHandle &G, void *x_pyq, const void *b_pyq, const SolveParam
     if (prm.solver == 1 && !info.fallback) {
       info.status = ST_RUNNING;
       run_gcr(dP, d64, w, vs, prm, tol2, info);
-      if (prm.precond != 0) nn_check(*prm.nn);
+      if (prm.precond == 1 || prm.precond == 2) nn_check(*prm.nn);
       if ((info.status == ST_STALLED || info.status == ST_BREAKDOWN || info.status == ST_NAN) &&
           info.iterations < prm.maxiter) {
         // the plain solver finishes: FP64 BiCGSTAB from the last FP64 iterate

@@ -41,8 +41,10 @@ struct SolveParams {
   double inner_tol = 0.1;   // GCR: inner solve stops at |r| <= inner_tol |r_outer|
   int gcr_k = 8;            // GCR: directions kept before a restart (<= 16)
   int gauge_precision = 0;  // 0: links stored like the spinors; 16 with precision 32: 16-bit links
-  int precond = 0;          // GCR: 0 inner BiCGSTAB, 1 network, 2 network then inner BiCGSTAB
+  int precond = 0;          // GCR: 0 inner BiCGSTAB, 1 network, 2 network then inner BiCGSTAB,
+                            // 3 multigrid coarse-grid correction then inner BiCGSTAB
   struct NNet *nn = nullptr;
+  struct MG *mg = nullptr;  // precond 3: built on the same handle and kappa
 };
 
 struct SolveInfo {

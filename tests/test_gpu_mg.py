@@ -95,3 +95,28 @@ def test_mg_zero_source_and_bad_parameters(q):
                     {"geo_block_size": [2, 2, 2, 2]}, {"n_vec": 17}, {"gcr_k": 0}):
             with pytest.raises(q.QcuError):
                 q.Multigrid(G, 0.12, **bad)
+
+
+@pytest.mark.parametrize("clover", [False, True])
+def test_gcr_with_coarse_grid_correction(q, clover):
+    """solve()'s precond 3: the coarse-grid correction of the multigrid, then
+    the inner 16-bit BiCGSTAB, inside the FP64 flexible GCR on M_pc."""
+    latt = [8, 8, 8, 16]
+    U = O.gauge_smooth(latt, 0.3, 21)
+    b = O.fermion_gauss(O.full_shape(latt), 121)
+    kappa = 0.124
+    c = kappa if clover else 0.0
+    A = [O.clover_build(U, latt, p, c) for p in (0, 1)] if clover else [None, None]
+    with q.Gauge(dev(U), latt, t_boundary=-1.0, clover_coeff=c) as G:
+        mg = q.Multigrid(G, kappa, n_vec=8, setup_maxiter=32, coarse_tol=0.05, coarse_maxiter=50)
+        x = empty_like_dev(O.full_shape(latt))
+        info = G.invert(x, dev(b), kappa, tol=1e-10, maxiter=20000, precision=16, solver="gcr", inner_iters=32,
+                        inner_tol=0.1, gcr_k=4, clover=clover, precond=3, mg=mg)
+        assert info["status"] == 1 and not info["fallback"], info
+        assert _true_residual(host(x), b, U, latt, kappa, -1.0, A) <= 1e-10
+        # the multigrid belongs to this handle and kappa: anything else is refused
+        with pytest.raises(q.QcuError):
+            G.invert(x, dev(b), kappa * 0.99, tol=1e-10, solver="gcr", clover=clover, precond=3, mg=mg)
+        with pytest.raises(q.QcuError):
+            G.invert(x, dev(b), kappa, tol=1e-10, solver="gcr", clover=clover, precond=3)
+        mg.close()
