@@ -20,8 +20,10 @@ and four more), the hopping-term bandwidth per storage and its roofline, the
 end-to-end time through the C ABI from host buffers, the clover target
 (32^3 x 64, csw 1, near-critical kappa), the 24^3 x 48 clover workload at
 every storage precision with errors against the CPU oracle's FP64 solve, the
-learned preconditioner, the batched multi-RHS solve, and a CPU baseline (the
-FP64 CPU oracle on all host cores, bounded sample).
+learned preconditioner, the batched multi-RHS solve, the two-level
+multigrid (set-up, its own solve, and the chosen solver with its coarse-grid
+correction), and a CPU baseline (the FP64 CPU oracle on all host cores,
+bounded sample).
 
 `--impl reference` times one complete FP64 solve of the CPU restatement of
 qcu's algorithm on the same system, measured, beside qcu's own GPU kernels
@@ -431,6 +433,43 @@ def clover_target(args, q, gauge, b, x, latt, stream, chosen_kw):
             "speedup_vs_plain_fp64": round(tp / tc, 3)}
 
 
+def multigrid_block(args, q, G, b, x, stream, chosen_kw):
+    """Two-level multigrid on the benchmark system (Wilson, kappa 0.1303):
+    set-up (12 near-null vectors from 200 FP32 BiCGSTAB iterations each, 4^4
+    aggregates), then one timed solve to the same 1e-10 true residual with
+    the multigrid alone (FP64 flexible GCR around the two-level cycle) and
+    one with the chosen solver whose GCR step first applies the coarse-grid
+    correction (precond 3); each after a warm-up solve."""
+    mg = q.Multigrid(G, args.kappa, n_vec=12, setup_maxiter=200, nu_post=4, coarse_tol=0.05, coarse_maxiter=50)
+    try:
+        def mg_solve():
+            info = mg.invert(x, b, tol=TOL, maxiter=1000)
+            if info["status"] != 1 or info["true_residual"] > TOL:
+                raise RuntimeError(f"multigrid solve failed: {info}")
+            return info
+        def pc_solve():
+            info = G.invert(x, b, args.kappa, tol=TOL, maxiter=20000, **{**chosen_kw, "solver": "gcr"}, precond=3, mg=mg)
+            if info["status"] != 1 or info["true_residual"] > TOL:
+                raise RuntimeError(f"coarse-corrected solve failed: {info}")
+            return info
+        mg_solve()
+        tm, im = event_time(stream, mg_solve)
+        pc_solve()
+        tp, ip = event_time(stream, pc_solve)
+        orth, gal = mg.check()
+        return {"workload": "wilson-bicgstab-32^3x64-smooth-eps0.25", "kappa": args.kappa,
+                "params": {"geo_block_size": [4, 4, 4, 4], "n_vec": 12, "setup_maxiter": 200, "nu_pre": 0,
+                           "nu_post": 4, "coarse_tol": 0.05, "coarse_maxiter": 50, "gcr_k": 8},
+                "setup_seconds": round(mg.setup_seconds, 3), "orthonormality_err": orth, "galerkin_err": gal,
+                "mg_solve": {"seconds": round(tm, 4), "outer_steps": im["outer"], "coarse_iterations": im["coarse_iters"],
+                             "true_residual": im["true_residual"]},
+                "chosen_with_coarse_correction": {"seconds": round(tp, 4), "iterations": ip["iterations"],
+                                                  "outer_steps": ip["reliable_updates"],
+                                                  "true_residual": ip["true_residual"]}}
+    finally:
+        mg.close()
+
+
 def batch_config(args, q, stream, chosen_kw):
     """Batched multi-RHS workload: the 12 point sources of a propagator on
     32^3 x 64 clover (csw = 1) together with 4 Gaussian right-hand sides on
@@ -789,6 +828,7 @@ def run_ours(args, world, rank, local, pg):
         extra["clover_24x24x24x48"] = clover_c3_block(q, lib_stream)
         extra["learned"] = learned_block(q, lib_stream, chosen_kw, gauge, b, latt)
         extra["batch"] = batch_config(args, q, lib_stream, chosen_kw)
+        extra["multigrid"] = multigrid_block(args, q, G, b, x, lib_stream, chosen_kw)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -6,6 +6,7 @@
     python -m qcu_b200.perf precisions
     python -m qcu_b200.perf legacy --iters 20
     python -m qcu_b200.perf nn --iters 20
+    python -m qcu_b200.perf mg --n-vec 12 --setup-maxiter 200
 
 `dslash` applies the even-odd hopping term `iters` times (after 3 warm-up
 launches) on a seeded smooth gauge field and prints the time per launch and
@@ -21,7 +22,10 @@ fields, one kernel per call) `iters` times and prints the wall time per
 synchronous call.  `nn` applies the learned preconditioner's network
 (random weights, scale 0.3) `iters` times on an odd half spinor and prints
 the time per application with the tensor-core layers and with the FP32 FMA
-layers.  `precisions` solves one system (default: the benchmark's) with plain
+layers.  `mg` sets up the two-level multigrid (--n-vec near-null vectors from
+--setup-maxiter iterations, 4^4 aggregates, nu_post 4, coarse tolerance 0.05
+with at most 50 iterations) and solves M x = b once with it, printing the
+set-up time and the solver report.  `precisions` solves one system (default: the benchmark's) with plain
 FP64 BiCGSTAB, BiCGSTAB with FP64 reliable updates at 32 and 16 bits, and
 the FP64 GCR around 32- and 16-bit inner solves, and states each solution's
 difference from the FP64 one.  Inputs are
@@ -52,7 +56,9 @@ def _gauge(latt, eps, seed, t_bc, csw=0.0, kappa=0.0):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["dslash", "solve", "batch", "precisions", "legacy", "nn"])
+    ap.add_argument("what", choices=["dslash", "solve", "batch", "precisions", "legacy", "nn", "mg"])
+    ap.add_argument("--n-vec", type=int, default=12)
+    ap.add_argument("--setup-maxiter", type=int, default=200)
     ap.add_argument("--latt", type=int, nargs=4, default=[32, 32, 32, 64])
     ap.add_argument("--eps", type=float, default=0.25)
     ap.add_argument("--seed", type=int, default=20251203)
@@ -116,6 +122,23 @@ def main(argv=None):
             res[name + "_ms_per_apply"] = round(e0.elapsed_time(e1) / a.iters, 4)
         print(json.dumps(res))
         net.close()
+        G.close()
+        return
+    if a.what == "mg":
+        G, u, L = _gauge(a.latt, a.eps, a.seed, a.t_bc, a.csw, a.kappa)
+        del u
+        b = torch.empty(L.full, dtype=torch.complex128, device="cuda")
+        q.fermion_random(b, b.numel(), 0, 7)
+        x = torch.empty_like(b)
+        mg = q.Multigrid(G, a.kappa, n_vec=a.n_vec, setup_maxiter=a.setup_maxiter, nu_post=4, coarse_tol=0.05,
+                         coarse_maxiter=50)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        info = mg.invert(x, b, tol=a.tol, maxiter=1000)
+        torch.cuda.synchronize()
+        print(json.dumps({"kernel": "mg", "latt": a.latt, "kappa": a.kappa, "setup_s": round(mg.setup_seconds, 3),
+                          "solve_s": round(time.perf_counter() - t0, 4), **info}))
+        mg.close()
         G.close()
         return
     if a.what == "legacy":
