@@ -55,7 +55,8 @@ __device__ __forceinline__ void link_at(const GaugeView<GAOS64> &U, const Geom &
 
 // sum of the four leaves in plane (mu, nu) at c[] (same products as qcu, in the
 // same left-to-right order)
-__device__ void clover_leaves(const GaugeView<GAOS64> &U, const Geom &g, const int c[4], int mu, int nu, C *Q) {
+__device__ __noinline__ void clover_leaves(const GaugeView<GAOS64> &U, const Geom &g, const int c[4], int mu, int nu,
+                                           C *Q) {
   int a[4], b[4];
   C u1[9], u2[9], u3[9], u4[9], t[9];
 #define SH(dst, src, d, st)                 \
@@ -144,31 +145,42 @@ __device__ __forceinline__ void block_store(void *out, int blk, int s, const C M
 __device__ bool herm6_inverse(const C A[36], C Ai[36]) {
   C L[36];
   double D[6];
+#pragma unroll
   for (int j = 0; j < 6; j++) {
     double dj = A[j * 6 + j].re;
+#pragma unroll
     for (int k = 0; k < j; k++) dj -= L[j * 6 + k].norm2() * D[k];
     if (dj == 0.0 || !(dj == dj)) return false;
     D[j] = dj;
+#pragma unroll
     for (int i = j + 1; i < 6; i++) {
       C v = A[i * 6 + j];
+#pragma unroll
       for (int k = 0; k < j; k++) v -= L[i * 6 + k] * L[j * 6 + k].conj() * D[k];
       L[i * 6 + j] = v * (1.0 / dj);
     }
   }
   // M = L^-1 (unit lower triangular)
   C M[36];
+#pragma unroll
   for (int j = 0; j < 6; j++) {
+#pragma unroll
     for (int i = 0; i < 6; i++) M[i * 6 + j] = C(i == j ? 1.0 : 0.0, 0.0);
+#pragma unroll
     for (int i = j + 1; i < 6; i++) {
       C v(0, 0);
+#pragma unroll
       for (int k = j; k < i; k++) v += L[i * 6 + k] * M[k * 6 + j];
       M[i * 6 + j] = -v;
     }
   }
   // A^-1 = M^H D^-1 M
+#pragma unroll
   for (int i = 0; i < 6; i++)
+#pragma unroll
     for (int j = 0; j <= i; j++) {
       C v(0, 0);
+#pragma unroll
       for (int k = i; k < 6; k++) v += M[k * 6 + i].conj() * M[k * 6 + j] * (1.0 / D[k]);
       Ai[i * 6 + j] = v;
       Ai[j * 6 + i] = v.conj();
@@ -187,25 +199,39 @@ __global__ void k_clover_build(Geom g, GaugeView<GAOS64> U, int par, double coef
   const int z = r % g.Lz;
   const int t = r / g.Lz;
   const int c[4] = {2 * xh + ((y + z + t + par) & 1), y, z, t};
+  // every loop below is unrolled, so blk is indexed at compile time and
+  // stays in registers (a runtime index would place it in local memory)
   C blk[2][36];
+#pragma unroll
   for (int b = 0; b < 2; b++)
+#pragma unroll
     for (int k = 0; k < 36; k++) blk[b][k] = C(0, 0);
+#pragma unroll
   for (int mu = 0; mu < 4; mu++)
+#pragma unroll
     for (int nu = mu + 1; nu < 4; nu++) {
       C Q[9], F[9];
       clover_leaves(U, g, c, mu, nu, Q);
+#pragma unroll
       for (int i = 0; i < 3; i++)
+#pragma unroll
         for (int k = 0; k < 3; k++) F[i * 3 + k] = Q[i * 3 + k] - Q[k * 3 + i].conj();
+#pragma unroll
       for (int s0 = 0; s0 < 4; s0++) {
         const int j = gcol(mu, s0), s1 = gcol(nu, j);
         const C sv = unit(gre(mu, s0), gim(mu, s0)) * unit(gre(nu, j), gim(nu, j));
         const int b = s0 >> 1, r0 = (s0 & 1) * 3, c0 = (s1 & 1) * 3;
+#pragma unroll
         for (int i = 0; i < 3; i++)
+#pragma unroll
           for (int k = 0; k < 3; k++) blk[b][(r0 + i) * 6 + c0 + k] += sv * F[i * 3 + k];
       }
     }
+#pragma unroll
   for (int b = 0; b < 2; b++) {
+#pragma unroll
     for (int k = 0; k < 36; k++) blk[b][k] = blk[b][k] * (-0.125 * coeff);
+#pragma unroll
     for (int k = 0; k < 6; k++) blk[b][k * 7] += C(1.0, 0.0);
     if (A64) block_store(A64, b, s, blk[b]);
     if (Ainv64) {
