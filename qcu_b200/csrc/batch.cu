@@ -87,12 +87,8 @@ __device__ __forceinline__ float wilson_hop_group2(Site2 (&acc)[NR], const Spino
 #pragma unroll
     for (int c = 0; c < 3; c++)
       acc[j].up.re[c] = acc[j].up.im[c] = acc[j].lo.re[c] = acc[j].lo.im[c] = make_float2(0.f, 0.f);
-  const int xh = s % g.Lxh;
-  int r = s / g.Lxh;
-  const int y = r % g.Ly;
-  r /= g.Ly;
-  const int z = r % g.Lz;
-  const int t = r / g.Lz;
+  int xh, y, z, t;
+  site_coords(g, s, xh, y, z, t);
   const int xodd = (y + z + t + par) & 1;
   float unit = 1.0f;
   auto hop = [&](auto mu_c, auto fwd_c, int n, int lpar, int ls, float ph) {
@@ -104,11 +100,11 @@ __device__ __forceinline__ float wilson_hop_group2(Site2 (&acc)[NR], const Spino
     for (int j = 0; j < NR; j++) {  // every slot is computed; closed slots read a valid buffer
       Site2 psi;
       if constexpr (K == SOA16) {
-        const float f = ph * site16_load_biased(in[j], n, psi) * (1.0f / FIX16_SCALE);
-        hop2<MU, FWD, true, true>(acc[j], psi, u, f);
+        const float f = ph * site16_load_biased<(MU < 2)>(in[j], n, psi) * (1.0f / FIX16_SCALE);
+        hop2<MU, FWD, true, true, link2_row2_raw<G>()>(acc[j], psi, u, f, LINK16_ROW2_F);
       } else {
         site2_load(in[j], n, psi);
-        hop2<MU, FWD, false>(acc[j], psi, u, ph);
+        hop2<MU, FWD, false, false, link2_row2_raw<G>()>(acc[j], psi, u, ph, LINK16_ROW2_F);
       }
     }
   };

@@ -135,7 +135,32 @@ struct Geom {
   int Lxh, Ly, Lz, Lt;
   int sy, sz, st;  // index strides of y, z, t
   int Vh;
+  // reciprocal multipliers of Lxh, Ly, Lz: n / d = umulhi(n, m) for every
+  // site index n (set by make_geom when that is exact, else 0: plain division)
+  unsigned m_lxh = 0, m_ly = 0, m_lz = 0;
 };
+
+// n / d for 0 <= n < 2^31.  With m = ceil(2^32 / d) = (2^32 + e) / d, 0 <= e < d,
+// n m / 2^32 = n / d + n e / (d 2^32), and the floor is exact while n e < 2^32
+// (division by invariant integers, Granlund and Montgomery 1994); the host sets
+// m only where Vh * d < 2^32 guarantees that, and 0 otherwise.
+__host__ __device__ __forceinline__ int geom_div(int n, int d, unsigned m) {
+#ifdef __CUDA_ARCH__
+  return m ? (int)__umulhi((unsigned)n, m) : n / d;
+#else
+  return n / d;
+#endif
+}
+
+// coordinates (xh, y, z, t) of site s of one parity
+__host__ __device__ __forceinline__ void site_coords(const Geom &g, int s, int &xh, int &y, int &z, int &t) {
+  const int r1 = geom_div(s, g.Lxh, g.m_lxh);
+  xh = s - r1 * g.Lxh;
+  const int r2 = geom_div(r1, g.Ly, g.m_ly);
+  y = r1 - r2 * g.Ly;
+  t = geom_div(r2, g.Lz, g.m_lz);
+  z = r2 - t * g.Lz;
+}
 
 // ------------------------------------------------------------------ spinors
 template <int K>

@@ -163,6 +163,15 @@ __device__ __forceinline__ float2 fix16_biased2(unsigned w) {
   return make_float2(__int_as_float(__byte_perm(w, 0x4B000000u, 0x7610)),
                      __int_as_float(__byte_perm(w, 0x4B000000u, 0x7632)));
 }
+// the same with the two halves exchanged: (spin b, spin a)
+__device__ __forceinline__ float2 fix16_biased2_swapped(unsigned w) {
+  return make_float2(__int_as_float(__byte_perm(w, 0x4B000000u, 0x7632)),
+                     __int_as_float(__byte_perm(w, 0x4B000000u, 0x7610)));
+}
+// SWAP_LO: the lower spins come as (spin 3, spin 2), the lane order in which
+// the x and y projections combine them with spins 0 and 1 (the byte permute
+// places each half where it is wanted, at no cost)
+template <bool SWAP_LO>
 __device__ __forceinline__ float site16_load_biased(const SpinorView<SOA16> &v, int s, Site2 &o) {
   unsigned w[12];
   s16_load_words(v.p, s, w);
@@ -170,8 +179,13 @@ __device__ __forceinline__ float site16_load_biased(const SpinorView<SOA16> &v, 
   for (int c = 0; c < 3; c++) {
     o.up.re[c] = fix16_biased2(w[2 * c]);
     o.up.im[c] = fix16_biased2(w[2 * c + 1]);
-    o.lo.re[c] = fix16_biased2(w[6 + 2 * c]);
-    o.lo.im[c] = fix16_biased2(w[6 + 2 * c + 1]);
+    if constexpr (SWAP_LO) {
+      o.lo.re[c] = fix16_biased2_swapped(w[6 + 2 * c]);
+      o.lo.im[c] = fix16_biased2_swapped(w[6 + 2 * c + 1]);
+    } else {
+      o.lo.re[c] = fix16_biased2(w[6 + 2 * c]);
+      o.lo.im[c] = fix16_biased2(w[6 + 2 * c + 1]);
+    }
   }
   return __ldg(v.norm + s);
 }
@@ -220,25 +234,43 @@ __device__ __forceinline__ void site_store2(const SpinorView<K> &v, int s, const
 }
 
 // ------------------------------------------------------------------ links
-// row 2 = conj(row0 x row1) times f, computed once in scalar FP32 (a paired
-// instruction takes the FMA pipe for two lanes, so a broadcast pair would
-// cost twice) and then broadcast (k = 3 * r + c)
-__device__ __forceinline__ void link2_row2(Link2 &m, float f) {
-  Cpx<float> r[9];
+// row 2 = conj(row0 x row1), each element as one FMUL and three FFMA per
+// component, then broadcast (k = 3 * r + c).  Scalar: a paired instruction
+// takes the FMA pipe for two lanes, so a broadcast pair would cost twice.
+__device__ __forceinline__ Cpx<float> conj_cross(const Cpx<float> &a, const Cpx<float> &b, const Cpx<float> &c,
+                                                 const Cpx<float> &d) {  // conj(a b - c d)
+  const float re = fmaf(a.re, b.re, fmaf(-a.im, b.im, fmaf(-c.re, d.re, c.im * d.im)));
+  const float im = fmaf(c.re, d.im, fmaf(c.im, d.re, fmaf(-a.re, b.im, -(a.im * b.re))));
+  return Cpx<float>(re, im);
+}
+__device__ __forceinline__ void link2_row2(Link2 &m) {
+  Cpx<float> r[6];
 #pragma unroll
   for (int k = 0; k < 6; k++) r[k] = Cpx<float>(m.re[k].x, m.im[k].x);
-  su3_row2(r);
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    m.re[6 + c] = bc2(r[6 + c].re * f);
-    m.im[6 + c] = bc2(r[6 + c].im * f);
-  }
+  const Cpx<float> r6 = conj_cross(r[1], r[5], r[2], r[4]);
+  const Cpx<float> r7 = conj_cross(r[2], r[3], r[0], r[5]);
+  const Cpx<float> r8 = conj_cross(r[0], r[4], r[1], r[3]);
+  m.re[6] = bc2(r6.re);
+  m.im[6] = bc2(r6.im);
+  m.re[7] = bc2(r7.re);
+  m.im[7] = bc2(r7.im);
+  m.re[8] = bc2(r8.re);
+  m.im[8] = bc2(r8.im);
 }
+
+// GSOA16 rows 0-1 are integers (units of 1/32767), so the rebuilt row 2 is
+// in units of 1/32767^2: the hop multiplies its share of the product by the
+// extra 1/32767 (hop2, R2F), on two lane pairs instead of six scalars.
+template <int G>
+constexpr bool link2_row2_raw() {
+  return G == GSOA16;
+}
+constexpr float LINK16_ROW2_F = 1.0f / FIX16_SCALE;
 
 // GSOA32: rows 0-1 as stored, row 2 rebuilt.  Returns the unit of the
 // elements (1).
-// GSOA16: rows 0-1 in units of 1/32767, row 2 rebuilt and brought to the same
-// unit.  Returns the unit (1/32767), applied once to the whole hop sum.
+// GSOA16: rows 0-1 in units of 1/32767, row 2 rebuilt in units of 1/32767^2.
+// Returns the unit of rows 0-1 (1/32767), applied once to the whole hop sum.
 template <int G>
 __device__ __forceinline__ float link2_load(const GaugeView<G> &u, int dir, int par, int s, Link2 &m) {
   const size_t slab = (size_t)(dir * 2 + par) * u.stride;
@@ -252,7 +284,7 @@ __device__ __forceinline__ float link2_load(const GaugeView<G> &u, int dir, int 
       m.re[2 * k + 1] = bc2(d.z);
       m.im[2 * k + 1] = bc2(d.w);
     }
-    link2_row2(m, 1.0f);
+    link2_row2(m);
     return 1.0f;
   } else {
     static_assert(G == GSOA16, "FP32 hop: GSOA32 or GSOA16 links");
@@ -264,7 +296,7 @@ __device__ __forceinline__ float link2_load(const GaugeView<G> &u, int dir, int 
       m.re[k] = bc2(a.x);
       m.im[k] = bc2(a.y);
     }
-    link2_row2(m, 1.0f / FIX16_SCALE);
+    link2_row2(m);
     return 1.0f / FIX16_SCALE;
   }
 }
@@ -276,12 +308,16 @@ __device__ __forceinline__ float link2_load(const GaugeView<G> &u, int dir, int 
 // SCALED.  Gamma conventions as gcol / gre / gim in fields.cuh.
 // BIASED: psi holds the biased values of a 16-bit spinor (site16_load_biased);
 // the projection returns exact values all the same.
-template <int MU, bool FWD, bool SCALED, bool BIASED = false>
-__device__ __forceinline__ void hop2(Site2 &acc, const Site2 &psi, const Link2 &u, float ph) {
+// R2F: row 2 of u is in units of r2f times those of rows 0-1 (link2_row2_raw).
+// With BIASED, the x and y hops (MU < 2) take psi with its lower spins
+// swapped (site16_load_biased<true>), so that their projection, too, runs
+// lane by lane.
+template <int MU, bool FWD, bool SCALED, bool BIASED = false, bool R2F = false>
+__device__ __forceinline__ void hop2(Site2 &acc, const Site2 &psi, const Link2 &u, float ph, float r2f = 1.0f) {
   constexpr int S = FWD ? -1 : 1;
   SpinPair h, uh;
   // rows 0, 1 of the projector: h_r = psi_r + S g(mu,r) psi_gcol(mu,r)
-  if constexpr (MU >= 2) {  // gcol = 2, 3: lane-aligned with the lower spins
+  if constexpr (MU >= 2 || BIASED) {  // lane-aligned: gcol = 2, 3, or 3, 2 against swapped lower spins
     constexpr int A0 = S * gre(MU, 0), A1 = S * gre(MU, 1), B0 = S * gim(MU, 0), B1 = S * gim(MU, 1);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -318,13 +354,19 @@ __device__ __forceinline__ void hop2(Site2 &acc, const Site2 &psi, const Link2 &
       }
     }
   }
+  // U^dag h takes row 2 of U with colour 2 of h only: its factor goes there
+  constexpr bool R2_ON_H = R2F && !FWD;
   if constexpr (MU == 3 || SCALED) {
     const float2 f = bc2(ph);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      h.re[c] = mul2(h.re[c], f);
-      h.im[c] = mul2(h.im[c], f);
+      const float2 fc = (R2_ON_H && c == 2) ? bc2(ph * r2f) : f;
+      h.re[c] = mul2(h.re[c], fc);
+      h.im[c] = mul2(h.im[c], fc);
     }
+  } else if constexpr (R2_ON_H) {
+    h.re[2] = mul2(h.re[2], bc2(r2f));
+    h.im[2] = mul2(h.im[2], bc2(r2f));
   }
   // colour product on both spins at once
 #pragma unroll
@@ -353,6 +395,12 @@ __device__ __forceinline__ void hop2(Site2 &acc, const Site2 &psi, const Link2 &
         im = fma2(u.re[c * 3 + r], h.im[c], im);
         re = fma2(u.im[c * 3 + r], h.im[c], re);
         im = fma2(neg2(u.im[c * 3 + r]), h.re[c], im);
+      }
+    }
+    if constexpr (R2F && FWD) {
+      if (r == 2) {  // U h takes row 2 of U in row 2 of the result only
+        re = mul2(re, bc2(r2f));
+        im = mul2(im, bc2(r2f));
       }
     }
     uh.re[r] = re;
@@ -394,10 +442,10 @@ __device__ __forceinline__ float hop2_from(Site2 &acc, const SpinorView<K> &in, 
                                            int lpar, int ls, float ph) {
   Site2 psi;
   Link2 u;
-  if constexpr (K == SOA16) ph *= site16_load_biased(in, n, psi) * (1.0f / FIX16_SCALE);
+  if constexpr (K == SOA16) ph *= site16_load_biased<(MU < 2)>(in, n, psi) * (1.0f / FIX16_SCALE);
   else site2_load(in, n, psi);
   const float unit = link2_load<G>(U, MU, lpar, ls, u);
-  hop2<MU, FWD, K == SOA16, K == SOA16>(acc, psi, u, ph);
+  hop2<MU, FWD, K == SOA16, K == SOA16, link2_row2_raw<G>()>(acc, psi, u, ph, LINK16_ROW2_F);
   return unit;
 }
 
@@ -412,12 +460,8 @@ __device__ __forceinline__ float wilson_hop_site2(Site2 &acc, const SpinorView<K
   for (int c = 0; c < 3; c++) {
     acc.up.re[c] = acc.up.im[c] = acc.lo.re[c] = acc.lo.im[c] = make_float2(0.f, 0.f);
   }
-  const int xh = s % g.Lxh;
-  int r = s / g.Lxh;
-  const int y = r % g.Ly;
-  r /= g.Ly;
-  const int z = r % g.Lz;
-  const int t = r / g.Lz;
+  int xh, y, z, t;
+  site_coords(g, s, xh, y, z, t);
   const int xodd = (y + z + t + par) & 1;
   int n;
   float unit;

@@ -51,6 +51,14 @@ Geom make_geom(const int latt[4]) {
   g.sz = g.Lxh * g.Ly;
   g.st = g.Lxh * g.Ly * g.Lz;
   g.Vh = (int)vh;
+  // reciprocal multipliers, exact for every site index while Vh * d < 2^32 (geom_div)
+  auto magic = [&](int d) -> unsigned {
+    if (d < 2 || (uint64_t)(vh + 64) * (uint64_t)d >= (1ULL << 32)) return 0u;  // padded indices too
+    return (unsigned)(((1ULL << 32) + (uint64_t)d - 1) / (uint64_t)d);
+  };
+  g.m_lxh = magic(g.Lxh);
+  g.m_ly = magic(g.Ly);
+  g.m_lz = magic(g.Lz);
   return g;
 }
 
