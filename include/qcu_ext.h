@@ -127,6 +127,27 @@ typedef struct {
 int qcuInvertBatch(const qcuBatchSystem *systems, int n_systems, const qcuInvertParam *p, qcuInvertResult *results,
                    qcuBatchTune *tune);
 
+/* Timing of the batched solver's inner hopping kernel (no counterpart in
+ * qcu): the odd halves of every b_j are stored in the inner precision and the
+ * kernel of the first half of M_pc runs `iters` times on them; *ms = mean
+ * device time per launch (CUDA events).  tune: null or dslash_threads <= 0 =
+ * let the autotuner choose (the choice is written back); else that shape. */
+int qcuBatchDslashTime(const qcuBatchSystem *systems, int n_systems, int precision, int gauge_precision,
+                       qcuBatchTune *tune, int iters, double *ms);
+
+/* Multi-right-hand-side hopping term on the tcgen05 tensor cores (no
+ * counterpart in qcu, whose dslash takes one spinor): out_j = D_{parity <-
+ * 1-parity} in_j for j < nrhs (1..128), in/out = nrhs half spinors back to
+ * back ([nrhs][Vh][4][3] complex128, PyQuda layout, device).  Per site and
+ * hop one tensor-core product serves every right-hand side: spinors are
+ * rounded to FP16 once, B = real form of (1 -+ gamma_mu) x U in FP16 (from the
+ * 16-bit links), FP32 accumulation; the result is rounded to FP16 (about
+ * 1e-3 relative, against 1e-6 for the FP32 hop). */
+int qcuDslashMultiTC(qcuGauge h, void *out, const void *in, int nrhs, int parity);
+/* its kernel alone, on resident seeded multi-rhs fields: *ms = mean device
+ * time per application over `iters` launches (CUDA events) */
+int qcuDslashMultiTCTime(qcuGauge h, int nrhs, int parity, int iters, double *ms);
+
 /* Operator check of the batched solver's inner kernels (no counterpart in
  * qcu, whose solver takes one right-hand side).  For every right-hand side j
  * of every system, the odd half b_o of b_j is stored in the inner precision

@@ -166,6 +166,10 @@ _lib.qcuInvertParamDefault.restype = None
 _lib.qcuInvert.argtypes = [_vp, _vp, _vp, ctypes.POINTER(QcuInvertParam), ctypes.POINTER(QcuInvertResult)]
 _lib.qcuInvertBatch.argtypes = [ctypes.POINTER(QcuBatchSystem), ctypes.c_int, ctypes.POINTER(QcuInvertParam),
                                 ctypes.POINTER(QcuInvertResult), ctypes.POINTER(QcuBatchTune)]
+_lib.qcuBatchDslashTime.argtypes = [ctypes.POINTER(QcuBatchSystem), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+_lib.qcuDslashMultiTC.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
+_lib.qcuDslashMultiTCTime.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
 _lib.qcuBatchApplyMatPC.argtypes = [ctypes.POINTER(QcuBatchSystem), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.POINTER(QcuBatchTune), ctypes.c_void_p]
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -317,6 +321,18 @@ class Gauge:
         with 16-bit links (3216)."""
         _check(_lib.qcuDslash(self._h, _ptr(out), _ptr(inp), int(parity), int(clover), int(precision)))
 
+    def dslash_multi_tc(self, out, inp, nrhs: int, parity: int):
+        """out_j = D in_j for nrhs half spinors back to back ([nrhs][Vh][4][3]
+        complex128), on the tcgen05 tensor cores (FP16 operands, FP32
+        accumulation; qcuDslashMultiTC)."""
+        _check(_lib.qcuDslashMultiTC(self._h, _ptr(out), _ptr(inp), int(nrhs), int(parity)))
+
+    def dslash_multi_tc_time(self, nrhs: int, parity: int = 0, iters: int = 20) -> float:
+        """ms per application of the tensor-core multi-rhs kernel on resident fields."""
+        ms = ctypes.c_double()
+        _check(_lib.qcuDslashMultiTCTime(self._h, int(nrhs), int(parity), int(iters), ctypes.byref(ms)))
+        return ms.value
+
     def matpc(self, out, inp, kappa: float, clover: bool = False):
         _check(_lib.qcuMatPC(self._h, _ptr(out), _ptr(inp), float(kappa), int(clover)))
 
@@ -415,6 +431,26 @@ def batch_apply_matpc(systems, precision: int = 16, gauge_precision: int = 0, ds
     _check(_lib.qcuBatchApplyMatPC(sys_arr, len(systems), int(precision), int(gauge_precision), ctypes.byref(tune),
                                    dots.ctypes.data))
     return dots[:nrhs]
+
+
+def batch_dslash_time(systems, precision: int = 16, gauge_precision: int = 0, iters: int = 20, tune=None):
+    """ms per launch of the batched solver's inner hopping kernel (first half
+    of M_pc on the odd halves of every b), timed with CUDA events
+    (qcuBatchDslashTime).  tune: None = the autotuner's choice, else a dict
+    with dslash_threads, dslash_rhs, mma (and blas_sites).  Returns (ms, the
+    tunables used as a dict)."""
+    sys_arr, _ = _batch_systems(systems)
+    t = QcuBatchTune()
+    if tune is not None:
+        t.dslash_threads = int(tune["dslash_threads"])
+        t.dslash_rhs = int(tune["dslash_rhs"])
+        t.mma = int(tune.get("mma", 0))
+        t.blas_sites = int(tune.get("blas_sites", 256))
+    ms = ctypes.c_double()
+    _check(_lib.qcuBatchDslashTime(sys_arr, len(systems), int(precision), int(gauge_precision), ctypes.byref(t),
+                                   int(iters), ctypes.byref(ms)))
+    return ms.value, {"dslash_threads": t.dslash_threads, "dslash_rhs": t.dslash_rhs, "mma": t.mma,
+                      "blas_sites": t.blas_sites}
 
 
 # ---------------------------------------------------------------- several GPUs

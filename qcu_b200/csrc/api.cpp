@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "batch.h"
+#include "mrhs.h"
 #include "dd.h"
 #include "mg.h"
 #include "nn.h"
@@ -265,6 +266,55 @@ int qcuInvertBatch(const qcuBatchSystem *systems, int n_systems, const qcuInvert
     tune->blas_sites = t.blas_sites;
     tune->mma = t.mma;
   }
+  QCU_API_END
+}
+
+int qcuBatchDslashTime(const qcuBatchSystem *systems, int n_systems, int precision, int gauge_precision,
+                       qcuBatchTune *tune, int iters, double *ms) {
+  QCU_API_BEGIN
+  require(systems != nullptr && ms != nullptr && n_systems > 0, "null systems/ms pointer or no systems");
+  std::vector<BatchSystem> sys(n_systems);
+  for (int i = 0; i < n_systems; i++) {
+    require(systems[i].gauge != nullptr, "batch: null gauge handle");
+    sys[i].G = systems[i].gauge->h;
+    sys[i].nrhs = systems[i].nrhs;
+    sys[i].kappa = systems[i].kappa;
+    sys[i].use_clover = systems[i].use_clover;
+    sys[i].x = systems[i].x;
+    sys[i].b = systems[i].b;
+  }
+  SolveParams p;
+  p.precision = precision;
+  p.gauge_precision = gauge_precision;
+  BatchTune t, chosen;
+  const bool force = tune != nullptr && tune->dslash_threads > 0;
+  if (force) {
+    t.dslash_threads = tune->dslash_threads;
+    t.dslash_rhs = tune->dslash_rhs;
+    t.blas_sites = tune->blas_sites;
+    t.mma = tune->mma;
+  }
+  solve_batch(sys, p, &chosen, force ? &t : nullptr, nullptr, ms, iters);
+  if (tune) {
+    tune->dslash_threads = chosen.dslash_threads;
+    tune->dslash_rhs = chosen.dslash_rhs;
+    tune->blas_sites = chosen.blas_sites;
+    tune->mma = chosen.mma;
+  }
+  QCU_API_END
+}
+
+int qcuDslashMultiTC(qcuGauge h, void *out, const void *in, int nrhs, int parity) {
+  QCU_API_BEGIN
+  require(h != nullptr, "null gauge handle");
+  handle_dslash_mrhs(*h->h, out, in, nrhs, parity);
+  QCU_API_END
+}
+
+int qcuDslashMultiTCTime(qcuGauge h, int nrhs, int parity, int iters, double *ms) {
+  QCU_API_BEGIN
+  require(h != nullptr && ms != nullptr, "null gauge handle or ms pointer");
+  *ms = handle_dslash_mrhs_time(*h->h, nrhs, parity, iters);
   QCU_API_END
 }
 

@@ -130,7 +130,11 @@ struct BatchSystem {
 // force_tune: use these tunables (no autotuning).  apply_dots: instead of
 // solving, apply the batched inner operator once per rhs (apply mode, below)
 // and write 5 doubles per rhs there.
+// dslash_ms: instead of solving, time the inner hopping kernel (first half of
+// M_pc on the odd halves of b, dslash_iters launches, CUDA events) and write
+// the mean time per launch there.
 std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const SolveParams &prm, BatchTune *tune_out,
-                                   const BatchTune *force_tune = nullptr, double *apply_dots = nullptr);
+                                   const BatchTune *force_tune = nullptr, double *apply_dots = nullptr,
+                                   double *dslash_ms = nullptr, int dslash_iters = 0);
 
 }  // namespace qcu

@@ -73,7 +73,8 @@ std::vector<int2> make_tiles(const std::vector<int> &unit_vh, int sites) {
 }  // namespace
 
 std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const SolveParams &prm, BatchTune *tune_out,
-                                   const BatchTune *force_tune, double *apply_dots) {
+                                   const BatchTune *force_tune, double *apply_dots, double *dslash_ms,
+                                   int dslash_iters) {
   const auto t0 = std::chrono::steady_clock::now();
   require(!sys.empty(), "batch: no systems");
   require(prm.maxiter > 0 && prm.inner_iters > 0 && prm.gcr_k > 0, "batch: maxiter, inner_iters, gcr_k must be > 0");
@@ -366,6 +367,34 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
     set_launch_count(launches0);  // tuning launches are not part of the solve
   }
   if (tune_out) *tune_out = tune;
+
+  // ---- timing mode: the inner hopping kernel alone, on the odd halves of b
+  if (dslash_ms) {
+    require(dslash_iters >= 1, "batch dslash timing: iters must be positive");
+    for (int r = 0; r < R; r++) {
+      const size_t half = spinor_bytes(AOS64, Vh[r]);
+      const void *bo = static_cast<const char *>(rl[r].s->b) + 2 * half * rl[r].j + half;
+      RhsBufs &B = *c.rhs[r];
+      launch_convert(AOS64, kind, Vh[r], bo, nullptr, B.v[BV_P].data.p, B.v[BV_P].norm.as<float>(), st);
+    }
+    BDslOp d0;
+    d0.in = BV_P, d0.out = BV_TMP, d0.parity = 0, d0.clover = clov_any, d0.gate = BG_ALWAYS;
+    for (int i = 0; i < 3; i++) inner_dsl(d0);
+    cudaEvent_t e0, e1;
+    QCU_CUDA(cudaEventCreate(&e0));
+    QCU_CUDA(cudaEventCreate(&e1));
+    QCU_CUDA(cudaEventRecord(e0, st));
+    for (int i = 0; i < dslash_iters; i++) inner_dsl(d0);
+    QCU_CUDA(cudaEventRecord(e1, st));
+    QCU_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    QCU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *dslash_ms = (double)ms / dslash_iters;
+    for (int r = 0; r < R; r++) info[r].status = ST_CONVERGED;
+    return info;
+  }
 
   // ---- apply mode: the inner operator of the batched solve, once, as an
   //      operator (the kernels and launch shapes the inner iteration uses)

@@ -38,6 +38,7 @@
 #include <algorithm>
 
 #include "nn.h"
+#include "tc.cuh"
 
 namespace qcu {
 
@@ -64,75 +65,12 @@ struct TcShape {
 };
 
 constexpr int TC_THREADS = 128;
-constexpr unsigned TC_WAIT_LIMIT = 1u << 24;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// byte offset of element (row, k) in a K-major no-swizzle operand whose rows
-// hold `kpad` elements: 8-row x 8-element core matrices of 128 contiguous
-// bytes, adjacent along K (LBO = 128 B), then along rows (SBO = kpad / 8 * 128 B)
-__device__ __forceinline__ uint32_t kmajor_off(int row, int k, int kpad) {
-  return (uint32_t)((row >> 3) * (kpad / 8) * 128 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
-}
-
-// shared-memory matrix descriptor of tcgen05 (no swizzle)
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version of sm_100
-  return d;                // base offset 0, relative LBO, no swizzle
-}
 
 // instruction descriptor, kind::f16: BF16 A and B (K-major), FP32 D, M = 128
 template <int N>
 __device__ __forceinline__ uint32_t umma_idesc() {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  return umma_idesc_f16<128, N>(true);
 }
-
-__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                          uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (unsigned i = 0; i < TC_WAIT_LIMIT; i++) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (i > 64) __nanosleep(64);
-  }
-  return false;
-}
-
-// 16 consecutive FP32 columns of this warp's 32 tensor-memory lanes
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
-}
-
 
 // layouts of the layer inputs and outputs
 enum TcIo { TC_SOA64 = 0, TC_HID16 = 1 };
@@ -372,7 +310,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_nn_tc(TcArgs a, long long nsites
             const uint64_t ad = umma_desc(sA0 + buf * S::A_BYTES + c * S::A_COLOUR_BYTES + ks * 256, 128,
                                           S::KC / 8 * 128);
             const uint64_t bd = umma_desc(sB0 + (ch * S::KC / 16 + ks) * 256, 128, S::B_SBO);
-            umma_bf16(tmem + c * S::N, ad, bd, idesc, (ch > 0 || ks > 0) ? 1u : 0u);
+            umma_f16(tmem + c * S::N, ad, bd, idesc, (ch > 0 || ks > 0) ? 1u : 0u);
           }
         umma_commit(smem_u32(&bars[buf]));
       }

@@ -26,7 +26,10 @@ the time per application with the tensor-core layers and with the FP32 FMA
 layers.  `mg` sets up the two-level multigrid (--n-vec near-null vectors from
 --setup-maxiter iterations, 4^4 aggregates, nu_post 4, coarse tolerance 0.05
 with at most 50 iterations) and solves M x = b once with it, printing the
-set-up time and the solver report.  `precisions` solves one system (default: the benchmark's) with plain
+set-up time and the solver report.  `mrhs` times the multi-right-hand-side
+tensor-core hopping kernel (tcgen05, FP16 operands) against the batched FMA
+kernel (autotuned, FP32 spinors with 16-bit links and 16-bit spinors) on the
+same --nrhs right-hand sides of one system (the FMA one up to 64).  `precisions` solves one system (default: the benchmark's) with plain
 FP64 BiCGSTAB, BiCGSTAB with FP64 reliable updates at 32 and 16 bits, and
 the FP64 GCR around 32- and 16-bit inner solves, and states each solution's
 difference from the FP64 one.  Inputs are
@@ -57,7 +60,9 @@ def _gauge(latt, eps, seed, t_bc, csw=0.0, kappa=0.0):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["dslash", "solve", "batch", "precisions", "legacy", "nn", "mg"])
+    ap.add_argument("what", choices=["dslash", "solve", "batch", "precisions", "legacy", "nn", "mg", "mrhs"])
+    ap.add_argument("--nrhs", type=int, nargs="+", default=[12, 48, 64, 128], help="mrhs: right-hand-side counts")
+    ap.add_argument("--no-fma", action="store_true", help="mrhs: only the tensor-core kernel")
     ap.add_argument("--n-vec", type=int, default=12)
     ap.add_argument("--setup-maxiter", type=int, default=200)
     ap.add_argument("--latt", type=int, nargs=4, default=[32, 32, 32, 64])
@@ -126,6 +131,9 @@ def main(argv=None):
         net.close()
         G.close()
         return
+    if a.what == "mrhs":
+        _mrhs(a)
+        return
     if a.what == "mg":
         G, u, L = _gauge(a.latt, a.eps, a.seed, a.t_bc, a.csw, a.kappa)
         del u
@@ -182,6 +190,40 @@ def main(argv=None):
     if len(times) > 1:
         info["seconds_each"] = times  # the first includes graph capture; the median is of the others
     print(json.dumps(info))
+    G.close()
+
+
+def _mrhs(a):
+    """The multi-rhs hopping term: the tcgen05 kernel against the batched FMA
+    kernel (autotuned: sites per block, rhs per thread, the mma.sync path) on
+    the same right-hand sides of one system, per application and per
+    right-hand-side site."""
+    import torch
+
+    import qcu_b200 as q
+
+    G, u, L = _gauge(a.latt, a.eps, a.seed, a.t_bc)
+    del u
+    res = {"kernel": "mrhs", "latt": a.latt, "vh": L.vh, "rows": []}
+    for n in a.nrhs:
+        row = {"nrhs": n}
+        ms = G.dslash_multi_tc_time(n, 0, iters=a.iters)
+        # algorithmic bytes: FP16 in and out (48 B each per rhs-site) + 8 16-bit links per site
+        byts = L.vh * (96 * n + 8 * 24)
+        row["tc"] = {"ms": round(ms, 4), "ps_per_rhs_site": round(ms * 1e9 / (L.vh * n), 2),
+                     "GBps": round(byts / (ms * 1e-3) / 1e9, 1)}
+        if n <= 64 and not a.no_fma:
+            b = torch.empty((n,) + tuple(L.full), dtype=torch.complex128, device="cuda")
+            q.fermion_random(b, b.numel(), 0, 11)
+            x = torch.zeros_like(b)
+            for name, prec, gp in (("fma_fp32_links16", 32, 16), ("fma_16bit", 16, 0)):
+                ms2, tune = q.batch_dslash_time([(G, x, b, 0.12, False)], precision=prec, gauge_precision=gp,
+                                                iters=a.iters)
+                row[name] = {"ms": round(ms2, 4), "ps_per_rhs_site": round(ms2 * 1e9 / (L.vh * n), 2), "tune": tune}
+            del b, x
+            torch.cuda.empty_cache()
+        res["rows"].append(row)
+    print(json.dumps(res))
     G.close()
 
 
