@@ -22,24 +22,34 @@
 // of 8 rows x 16 B, LBO = 16 RP B between K-chunks, SBO = 128 B between
 // 8-row groups), so one bulk copy brings a neighbour's whole A tile.
 //
-// A CTA of 128 threads is persistent over sites, two in flight:
-//   * thread 0 issues, one site ahead, the 8 bulk copies (cp.async.bulk, no
-//     multicast) of the neighbours' A tiles, completing on the slot's mbarrier;
-//   * eight threads decode the 8 links (16-bit reconstruct-12), 72 threads
-//     write for every link element its signed and swapped FP16 pairs, and all
-//     threads assemble the 8 B matrices from those pairs (a 16-byte segment
-//     of a B row each; all-zero segments are never written);
-//   * thread 0 issues the site's 16 MMAs (kind::f16, M = 128, N = 32,
-//     K = 16; FP32 accumulators in tensor memory) and commits them;
-//   * the previous site's accumulators are read back (tcgen05.ld, one warp
-//     per 32 right-hand sides), rounded to FP16 and stored.
-// K runs to 32 per hop (24 used): B's columns 24-31 are zero, so the fourth
-// K-chunk of A (the next tile, or a zeroed pad after the last) adds nothing.
+// One CTA per SM, persistent over sites, with warp roles joined only by
+// mbarriers, so that loads, B builds, MMAs and read-back of different sites
+// overlap (3 or 4 site slots, four accumulator slots):
+//   * warps 0-3 load, running ahead of the others: per site the 8
+//     neighbours' A tiles as 16-byte cp.async pieces (a warp moves 512
+//     contiguous bytes per step; one bulk-copy engine per SM issued them
+//     ~8x slower) and the 8 links' 16-bit words, one cp.async group per
+//     site, released one site later (wait, proxy fence, arrive);
+//   * warps 4-7 decode the links (a thread per link element, row 2 rebuilt
+//     where taken), write for every element its signed and swapped FP16
+//     pairs, and assemble the B operand from those pairs (a 16-byte segment
+//     of a B row per thread; all-zero segments are never written);
+//   * one thread of warp 8 issues the site's 12 MMAs (kind::f16, M = 128,
+//     N = 32, K = 16; FP32 accumulators in tensor memory) and commits them
+//     to the slot (freeing it) and to the accumulator slot;
+//   * warps 9-12 read the accumulators back (tcgen05.ld, one warp per 32
+//     right-hand sides), round them to FP16 and store them.
+// The 8 neighbour tiles of a site lie back to back with one K-chunk stride
+// (chunk c of hop h at (3 h + c) LBO), so the site is a single GEMM with
+// K = 192: 12 MMAs of K = 16, B stored as one 32 x 192 operand (rows 24-31
+// zero).
 // With RP = 64 the MMA's rows 64-127 read neighbouring data; those rows of
 // D are never stored.  Sites are visited in z-slabs (every t of zb z-planes,
 // then the next slab), so the 8 reads of an input tile fall within a window
-// that L2 holds.  Every wait is bounded: a time-out sets the error flag,
-// stops the CTA and still frees its tensor memory.
+// that L2 holds.  Every wait is bounded and ends early once any role has
+// set the CTA's abort flag; a time-out sets the error flag, and the warps
+// that issued copies or MMAs wait (bounded) for them before the CTA frees
+// its tensor memory and exits.
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -53,38 +63,44 @@ namespace qcu {
 
 namespace {
 
-constexpr int MT_THREADS = 128;
+// roles: warps 0-3 load (the A tiles and the link words, by cp.async),
+// warps 4-7 build the B matrices, one thread of warp 8 issues the MMAs,
+// warps 9-12 read the accumulators back (tensor-memory lane quarters 1, 2,
+// 3, 0: warp w may access lanes 32 (w % 4) to 32 (w % 4) + 31)
+constexpr int MT_WARPS = 13;
+constexpr int MT_THREADS = MT_WARPS * 32;
+constexpr int MT_LOADERS = 128;  // warps 0-3
+constexpr int MT_BUILDERS = 128;  // warps 4-7
+constexpr int MT_BUILD_WARP0 = 4;
+constexpr int MT_MMA_WARP = 8;
 constexpr int MT_HOPS = 8;
-constexpr int MT_B_HOP = 32 * 32 * 2;  // one B matrix: 32 rows x K 32, FP16
-constexpr int MT_A_PAD = 2048;         // zeros read as the last hop's fourth K-chunk
+constexpr int MT_K = MT_HOPS * 24;       // K of a site's GEMM: 8 hops x 24 input components
+constexpr int MT_B_BYTES = 32 * MT_K * 2; // B: 32 rows (24 used) x K 192, FP16
 constexpr int MT_NVAR = MT_HOPS * 9 * 4;  // signed / swapped pairs of the link elements
 constexpr int MT_ZERO_WORD = MT_NVAR;     // index of a zero pair
 constexpr int MT_SEGS = MT_HOPS * 24 * 3;  // 16-byte B segments that can be non-zero
-constexpr int MT_SEG_SLOTS = (MT_SEGS + MT_THREADS - 1) / MT_THREADS;
+constexpr int MT_SEG_SLOTS = (MT_SEGS + MT_BUILDERS - 1) / MT_BUILDERS;
+constexpr int MT_ND = 4;                  // accumulator slots (32 tensor-memory columns each)
 
 template <int RP>
 struct MtShape {
   static constexpr int A_HOP = 48 * RP;  // bytes of one neighbour tile
-  static constexpr int A_BYTES = MT_HOPS * A_HOP + MT_A_PAD;
-  static constexpr int B_BYTES = MT_HOPS * MT_B_HOP;
-  static constexpr int SLOT = (A_BYTES + B_BYTES + 1023) / 1024 * 1024;
-  // shared: [slot 0 | slot 1] [V 8x9 float2] [pairs 8x9x4 + 4 words] [info x2] [2 + 2 mbarriers, tmem slot]
-  static constexpr int OFF_V = 2 * SLOT;
-  static constexpr int OFF_VAR = OFF_V + MT_HOPS * 9 * 8;
-  static constexpr int OFF_INFO = OFF_VAR + (MT_NVAR + 4) * 4;
-  static constexpr int OFF_BAR = OFF_INFO + 2 * 128;
-  static constexpr int SMEM = OFF_BAR + 64;
-  static constexpr int CTAS_PER_SM = RP == 64 ? 2 : 1;
+  static constexpr int A_BYTES = MT_HOPS * A_HOP;
+  static constexpr int B_BYTES = MT_B_BYTES;
+  // per site slot: [A tiles + pad][B matrices][link words 8 x 16 B][8 x 8 B][phases 8 x 4 B]
+  static constexpr int OFF_L16 = A_BYTES + B_BYTES;
+  static constexpr int OFF_L8 = OFF_L16 + MT_HOPS * 16;
+  static constexpr int OFF_PH = OFF_L8 + MT_HOPS * 8;
+  static constexpr int SLOT = (OFF_PH + MT_HOPS * 4 + 1023) / 1024 * 1024;
+  static constexpr int NS = RP == 64 ? 4 : 3;  // site slots (shared memory: 4 x 37 KB or 3 x 61 KB)
+  static constexpr int OFF_VAR = NS * SLOT;    // builders' scratch: the pairs of the 8 links' elements
+  static constexpr int OFF_BAR = OFF_VAR + (MT_NVAR + 4) * 4;
+  // mbarriers: full[NS] (A tiles + link words landed), bready[NS] (B built),
+  // mdone[NS] (the site's MMAs done: slot free), dfull[ND], dempty[ND]
+  static constexpr int NBAR = 3 * NS + 2 * MT_ND;
+  static constexpr int SMEM = OFF_BAR + NBAR * 8 + 16;  // + tensor-memory address, abort flag
+  static constexpr int EPI_WARPS = RP / 32;
 };
-
-// per site: the output site, the neighbour of each hop, the site and phase of each hop's link
-struct MtInfo {
-  int s;
-  int nbr[MT_HOPS];
-  int lsite[MT_HOPS];
-  float ph[MT_HOPS];
-};
-static_assert(sizeof(MtInfo) <= 128, "site info");
 
 struct MtArgs {
   Geom g;
@@ -95,47 +111,77 @@ struct MtArgs {
   int par;
   int zb;             // z-planes per slab of the visiting order
   int *err;
+  // reciprocal multipliers (geom_div) of Ly * Lxh, zb, Lt and Lxh, or 0: plain division
+  unsigned m_plane, m_zb, m_lt, m_lxh;
 };
 
-// q-th site of the visiting order: z-slabs of zb planes, t, then the planes of the slab, then (y, xh)
-__device__ __forceinline__ void mt_site_info(const MtArgs &a, int q, MtInfo &f) {
+// coordinates of the q-th site of the visiting order: z-slabs of zb planes,
+// then t, then the planes of the slab, then (y, xh)
+struct MtSite {
+  int s, xh, y, z, t;
+};
+__device__ __forceinline__ MtSite mt_site(const MtArgs &a, int q) {
   const Geom &g = a.g;
   const int plane = g.Ly * g.Lxh;
-  const int yx = q % plane;
-  int r = q / plane;
-  const int zz = r % a.zb;
-  r /= a.zb;
-  const int t = r % g.Lt;
-  const int z = (r / g.Lt) * a.zb + zz;
-  const int s = (t * g.Lz + z) * plane + yx;
-  const int xh = yx % g.Lxh, y = yx / g.Lxh;
-  const int xodd = (y + z + t + a.par) & 1;
-  f.s = s;
-  f.nbr[0] = xodd ? (xh == g.Lxh - 1 ? s - xh : s + 1) : s;
-  f.nbr[1] = xodd ? s : (xh == 0 ? s + g.Lxh - 1 : s - 1);
-  f.nbr[2] = (y == g.Ly - 1) ? s - (g.Ly - 1) * g.sy : s + g.sy;
-  f.nbr[3] = (y == 0) ? s + (g.Ly - 1) * g.sy : s - g.sy;
-  f.nbr[4] = (z == g.Lz - 1) ? s - (g.Lz - 1) * g.sz : s + g.sz;
-  f.nbr[5] = (z == 0) ? s + (g.Lz - 1) * g.sz : s - g.sz;
-  f.nbr[6] = (t == g.Lt - 1) ? s - (g.Lt - 1) * g.st : s + g.st;
-  f.nbr[7] = (t == 0) ? s + (g.Lt - 1) * g.st : s - g.st;
-#pragma unroll
-  for (int h = 0; h < MT_HOPS; h++) {
-    f.lsite[h] = (h & 1) ? f.nbr[h] : s;  // forward: U_mu(x); backward: U_mu(x - mu)
-    f.ph[h] = 1.f;
+  const int r1 = geom_div(q, plane, a.m_plane);
+  const int yx = q - r1 * plane;
+  const int r2 = geom_div(r1, a.zb, a.m_zb);
+  const int zz = r1 - r2 * a.zb;
+  const int zs = geom_div(r2, g.Lt, a.m_lt);
+  MtSite c;
+  c.t = r2 - zs * g.Lt;
+  c.z = zs * a.zb + zz;
+  c.s = (c.t * g.Lz + c.z) * plane + yx;
+  c.y = geom_div(yx, g.Lxh, a.m_lxh);
+  c.xh = yx - c.y * g.Lxh;
+  return c;
+}
+// neighbour of hop h (x+, x-, y+, y-, z+, z-, t+, t-) of output site c on parity par
+__device__ __forceinline__ int mt_nbr(const Geom &g, const MtSite &c, int par, int h) {
+  const int s = c.s, mu = h >> 1;
+  const bool fwd = (h & 1) == 0;
+  if (mu == 0) {  // even-odd x: the neighbour is s itself or s -+ 1 (wrapping within the row)
+    const int xodd = (c.y + c.z + c.t + par) & 1;
+    return fwd ? (xodd ? (c.xh == g.Lxh - 1 ? s - c.xh : s + 1) : s) : (xodd ? s : (c.xh == 0 ? s + g.Lxh - 1 : s - 1));
   }
-  if (t == g.Lt - 1) f.ph[6] = a.t_bc;
-  if (t == 0) f.ph[7] = a.t_bc;
+  const int x = mu == 1 ? c.y : (mu == 2 ? c.z : c.t);
+  const int L = mu == 1 ? g.Ly : (mu == 2 ? g.Lz : g.Lt);
+  const int st = mu == 1 ? g.sy : (mu == 2 ? g.sz : g.st);
+  return fwd ? (x == L - 1 ? s - (L - 1) * st : s + st) : (x == 0 ? s + (L - 1) * st : s - st);
 }
 
-__device__ __forceinline__ void bulk_expect(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
+// mbarrier wait bounded in iterations and ended early by the CTA's abort flag
+__device__ __forceinline__ bool mt_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag) {
+  for (unsigned i = 0; i < TC_WAIT_LIMIT; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((i & 63) == 63) {
+      if (*abort_flag) return false;
+      __nanosleep(32);
+    }
+  }
+  return false;
 }
+// AND of a predicate over the 128 builder threads (named barrier 1)
+__device__ __forceinline__ bool builders_and(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, 1, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v)
+      : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void builders_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t half2_bits(float lo, float hi) {
   const __half2 v = __floats2half2_rn(lo, hi);
@@ -162,216 +208,251 @@ __device__ __forceinline__ int mt_pair_word(int h, int n, int k2) {
 }
 
 template <int RP>
-__global__ void __launch_bounds__(MT_THREADS) k_mrhs_tc(MtArgs a) {
+__global__ void __launch_bounds__(MT_THREADS, 1) k_mrhs_tc(MtArgs a) {
   using S = MtShape<RP>;
+  constexpr int NS = S::NS;
   extern __shared__ __align__(1024) uint8_t smem[];
-  float2 *sV = reinterpret_cast<float2 *>(smem + S::OFF_V);
-  uint32_t *sVar = reinterpret_cast<uint32_t *>(smem + S::OFF_VAR);
-  MtInfo *sInfo = reinterpret_cast<MtInfo *>(smem + S::OFF_INFO);  // stride 128 B
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S::OFF_BAR);  // [0,1] A full, [2,3] MMAs done
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 4);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const Geom &g = a.g;
   const uint32_t s0 = smem_u32(smem);
-  auto info = [&](int slot) -> MtInfo & { return *reinterpret_cast<MtInfo *>(smem + S::OFF_INFO + slot * 128); };
-  (void)sInfo;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S::OFF_BAR);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + S::NBAR);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  auto bar_full = [&](int k) { return smem_u32(&bars[k]); };
+  auto bar_bready = [&](int k) { return smem_u32(&bars[NS + k]); };
+  auto bar_mdone = [&](int k) { return smem_u32(&bars[2 * NS + k]); };
+  auto bar_dfull = [&](int d) { return smem_u32(&bars[3 * NS + d]); };
+  auto bar_dempty = [&](int d) { return smem_u32(&bars[3 * NS + MT_ND + d]); };
+  auto fail = [&]() {
+    *abort_flag = 1;
+    atomicExch(a.err, 1);
+  };
 
-  // zero everything the MMAs may read before it is written (pads, zero columns of B)
+  // zero the slots (pads, the zero columns and rows of B) and the scratch
   for (int i = tid * 16; i < S::OFF_BAR; i += MT_THREADS * 16)
     *reinterpret_cast<uint4 *>(smem + i) = make_uint4(0u, 0u, 0u, 0u);
-  // this thread's B segments: table words of their four pairs and their offsets
-  int segw[MT_SEG_SLOTS][4];
-  int segoff[MT_SEG_SLOTS];
-  bool segon[MT_SEG_SLOTS];
-#pragma unroll
-  for (int m = 0; m < MT_SEG_SLOTS; m++) {
-    const int sg = tid + m * MT_THREADS;
-    segon[m] = false;
-    segoff[m] = 0;
-#pragma unroll
-    for (int p = 0; p < 4; p++) segw[m][p] = MT_ZERO_WORD;
-    if (sg < MT_SEGS) {
-      const int h = sg / 72, n = (sg % 72) / 3, j = sg % 3;
-#pragma unroll
-      for (int p = 0; p < 4; p++) {
-        segw[m][p] = mt_pair_word(h, n, 4 * j + p);
-        segon[m] = segon[m] || segw[m][p] != MT_ZERO_WORD;
-      }
-      segoff[m] = h * MT_B_HOP + (int)kmajor_off(n, 8 * j, 32);
+  if (tid == 0) {
+    *abort_flag = 0;
+    for (int k = 0; k < NS; k++) {
+      // every loader thread arrives once its copies for the site have landed
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_full(k)), "r"(MT_LOADERS) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_bready(k)), "r"(MT_BUILDERS / 32) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_mdone(k)) : "memory");
     }
+    for (int d = 0; d < MT_ND; d++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_dfull(d)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_dempty(d)), "r"(S::EPI_WARPS) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(64u)
+                 "r"(32u * MT_ND)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (tid == 0) {
-    for (int k = 0; k < 4; k++)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[k])) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // zeros visible to the async proxy
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the zeros, before any async write or read
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  const uint32_t idesc = umma_idesc_f16<128, 32>(false);
-  const GaugeView<GSOA16> U{a.gauge, pad_sites(g.Vh)};
   const int nloc = blockIdx.x < g.Vh ? (g.Vh - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-  auto a_addr = [&](int slot, int h) { return s0 + slot * S::SLOT + h * S::A_HOP; };
-  auto b_addr = [&](int slot, int h) { return s0 + slot * S::SLOT + S::A_BYTES + h * MT_B_HOP; };
-  // thread 0's count of what it issued and what it has seen complete, per
-  // slot: bulk-copy batches (A full) and MMA batches; the drain on an error
-  // waits for the difference
-  int a_iss[2] = {0, 0}, a_done[2] = {0, 0}, m_iss[2] = {0, 0}, m_done[2] = {0, 0};
-  // thread 0: site info of the i-th site and the bulk copies of its 8 A tiles
-  auto issue_site = [&](int i) {
-    const int slot = i & 1;
-    a_iss[slot]++;
-    MtInfo &f = info(slot);
-    mt_site_info(a, (int)blockIdx.x + i * (int)gridDim.x, f);
-    const uint32_t bar = smem_u32(&bars[slot]);
-    bulk_expect(bar, MT_HOPS * S::A_HOP);
-#pragma unroll
-    for (int h = 0; h < MT_HOPS; h++)
-      bulk_load(a_addr(slot, h), a.in + (size_t)f.nbr[h] * (24 * RP), S::A_HOP, bar);
-  };
-  if (tid == 0 && nloc > 0) issue_site(0);
-  __syncthreads();
+  auto q_of = [&](int i) { return (int)blockIdx.x + i * (int)gridDim.x; };
 
-  bool ok = true;
-  int s_prev = 0;
-  for (int i = 0; i < nloc && ok; i++) {
-    const int slot = i & 1;
-    // (1) the previous site's MMAs are done: its buffers are free and its accumulators ready
-    if (i >= 1) {
-      ok = mbar_wait(smem_u32(&bars[2 + (slot ^ 1)]), ((i - 1) >> 1) & 1);
-      if (ok) m_done[slot ^ 1]++;
-    }
-    // (2) one site ahead: info and A tiles of site i + 1 into the other slot
-    if (tid == 0 && ok && i + 1 < nloc) issue_site(i + 1);
-    // (3) B matrices of site i: links -> V, V -> signed / swapped pairs, pairs -> B segments
-    const MtInfo &f = info(slot);
-    const int s_cur = f.s;
-    if (tid < MT_HOPS) {
-      const int h = tid, mu = h >> 1;
-      const bool fwd = (h & 1) == 0;
-      const int lpar = fwd ? a.par : 1 - a.par;
-      unsigned w[6];
-      g16_load_words(U.p, (size_t)(mu * 2 + lpar) * U.stride, f.lsite[h], w);
-      Cpx<float> m[9];
-#pragma unroll
-      for (int k = 0; k < 6; k++) {
-        const float2 d = fix16_unpack(w[k]);
-        m[k] = Cpx<float>(d.x * (1.0f / FIX16_SCALE), d.y * (1.0f / FIX16_SCALE));
+  if (warp < MT_BUILD_WARP0) {
+    // ---------------------------------------------------------- loaders
+    // a site's 8 tiles are 8 x 3 RP pieces of 16 B; loader thread lt copies
+    // pieces lt, lt + 128, ...: a warp moves 512 contiguous bytes per step.
+    // Each site's copies are one cp.async group, released LAG sites later:
+    // wait for the group, fence (the tensor core reads what cp.async wrote),
+    // arrive on the slot's full barrier.
+    const int lt = tid;
+    constexpr int PIECES = MT_HOPS * 3 * RP, PER_TILE = 3 * RP;
+    // a site's group is released once the next site's copies are issued
+    // (a lag of 2 sites with 5 slots measured slower at 64 rows)
+    constexpr int LAG = 1;
+    auto release = [&](int k) {
+      asm volatile("cp.async.wait_group %0;" ::"n"(LAG) : "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(bar_full(k));
+    };
+    int i = 0;
+    for (; i < nloc; i++) {
+      const int k = i % NS, u = i / NS;
+      // the slot's previous site (i - NS) has finished its MMAs
+      if (u >= 1 && !__all_sync(0xffffffffu, mt_wait(bar_mdone(k), (u - 1) & 1, abort_flag))) {
+        if (lane == 0) fail();
+        break;
       }
-      m[6] = (m[1] * m[5] - m[2] * m[4]).conj();
-      m[7] = (m[2] * m[3] - m[0] * m[5]).conj();
-      m[8] = (m[0] * m[4] - m[1] * m[3]).conj();
-      const float ph = f.ph[h];
+      const MtSite c = mt_site(a, q_of(i));
+      uint8_t *slot = smem + k * S::SLOT;
+      const uint32_t sbase = s0 + k * S::SLOT;
+      int nbr[MT_HOPS];
 #pragma unroll
-      for (int r = 0; r < 3; r++)
+      for (int h = 0; h < MT_HOPS; h++) nbr[h] = mt_nbr(g, c, a.par, h);
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-          const Cpx<float> v = fwd ? m[r * 3 + c] : m[c * 3 + r].conj();
-          sV[h * 9 + r * 3 + c] = make_float2(v.re * ph, v.im * ph);
+      for (int j = 0; j < PIECES / MT_LOADERS; j++) {
+        const int pc = lt + j * MT_LOADERS;
+        const int h = pc / PER_TILE, off = (pc - h * PER_TILE) * 16;
+        const char *src = reinterpret_cast<const char *>(a.in) + (size_t)nbr[h] * (48 * RP) + off;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sbase + h * S::A_HOP + off), "l"(src)
+                     : "memory");
+      }
+      if (lt < MT_HOPS) {  // the link of hop h = lt: forward U_mu(x), backward U_mu(x - mu)
+        const int h = lt, mu = h >> 1;
+        const int lpar = (h & 1) ? 1 - a.par : a.par;
+        const int ls = (h & 1) ? nbr[h] : c.s;
+        const char *blk = static_cast<const char *>(a.gauge) + (size_t)(mu * 2 + lpar) * pad_sites(g.Vh) * 24 +
+                          (size_t)(ls >> 5) * G16_BLOCK_BYTES;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(slot + S::OFF_L16 + 16 * h)),
+                     "l"(blk + (ls & 31) * 16)
+                     : "memory");
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(slot + S::OFF_L8 + 8 * h)),
+                     "l"(blk + 512 + (ls & 31) * 8)
+                     : "memory");
+      }
+      if (lt == 0) {
+        float *ph = reinterpret_cast<float *>(slot + S::OFF_PH);
+#pragma unroll
+        for (int h = 0; h < MT_HOPS; h++) ph[h] = 1.f;
+        if (c.t == g.Lt - 1) ph[6] = a.t_bc;
+        if (c.t == 0) ph[7] = a.t_bc;
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      if (i >= LAG) release((i - LAG) % NS);
+    }
+    // the last sites' copies (and, after an abort, whatever is in flight)
+    // complete before the shared memory goes away
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (i == nloc)
+      for (int j = nloc - LAG < 0 ? 0 : nloc - LAG; j < nloc; j++) mbar_arrive(bar_full(j % NS));
+  } else if (warp < MT_MMA_WARP) {
+    // ---------------------------------------------------------- B builders
+    const int bt = tid - MT_BUILD_WARP0 * 32;
+    uint32_t *sVar = reinterpret_cast<uint32_t *>(smem + S::OFF_VAR);
+    int segw[MT_SEG_SLOTS][4];
+    int segoff[MT_SEG_SLOTS];
+    bool segon[MT_SEG_SLOTS];
+#pragma unroll
+    for (int m = 0; m < MT_SEG_SLOTS; m++) {
+      const int sg = bt + m * MT_BUILDERS;
+      segon[m] = false;
+      segoff[m] = 0;
+#pragma unroll
+      for (int p = 0; p < 4; p++) segw[m][p] = MT_ZERO_WORD;
+      if (sg < MT_SEGS) {
+        const int h = sg / 72, n = (sg % 72) / 3, j = sg % 3;
+#pragma unroll
+        for (int p = 0; p < 4; p++) {
+          segw[m][p] = mt_pair_word(h, n, 4 * j + p);
+          segon[m] = segon[m] || segw[m][p] != MT_ZERO_WORD;
         }
+        segoff[m] = S::A_BYTES + (int)kmajor_off(n, 24 * h + 8 * j, MT_K);
+      }
     }
-    __syncthreads();
-    if (tid < MT_HOPS * 9) {
-      const float2 v = sV[tid];
-      const uint32_t f0 = half2_bits(v.x, -v.y), f1 = half2_bits(v.y, v.x);
-      *reinterpret_cast<uint4 *>(sVar + tid * 4) = make_uint4(f0, f0 ^ 0x80008000u, f1, f1 ^ 0x80008000u);
-    }
-    __syncthreads();
-    const uint32_t bslot = (uint32_t)(slot * S::SLOT + S::A_BYTES);
+    for (int i = 0; i < nloc; i++) {
+      const int k = i % NS, u = i / NS;
+      bool ok = true;
+      if (bt < MT_HOPS) ok = mt_wait(bar_full(k), u & 1, abort_flag);
+      ok = builders_and(ok);
+      if (!ok) {
+        if (bt == 0) fail();
+        break;
+      }
+      const uint8_t *slot = smem + k * S::SLOT;
+      if (bt < MT_HOPS * 9) {  // element (r, cc) of V = phase x (U or U^dag) of hop h, as four FP16 pairs
+        const int h = bt / 9, e = bt - 9 * h, r = e / 3, cc = e - 3 * r;
+        const bool fwd = (h & 1) == 0;
+        const int ur = fwd ? r : cc, uc = fwd ? cc : r;  // the element of U it takes
+        auto word = [&](int w) {
+          return w < 4 ? reinterpret_cast<const uint32_t *>(slot + S::OFF_L16 + 16 * h)[w]
+                       : reinterpret_cast<const uint32_t *>(slot + S::OFF_L8 + 8 * h)[w - 4];
+        };
+        auto elem = [&](int w) {
+          const float2 d = fix16_unpack(word(w));
+          return Cpx<float>(d.x * (1.0f / FIX16_SCALE), d.y * (1.0f / FIX16_SCALE));
+        };
+        Cpx<float> v;
+        if (ur < 2) {
+          v = elem(ur * 3 + uc);
+        } else {  // row 2 = conj(row0 x row1)
+          const int b1 = uc == 2 ? 0 : uc + 1, b2 = uc == 0 ? 2 : uc - 1;
+          v = (elem(b1) * elem(3 + b2) - elem(b2) * elem(3 + b1)).conj();
+        }
+        if (!fwd) v = v.conj();
+        const float ph = reinterpret_cast<const float *>(slot + S::OFF_PH)[h];
+        const uint32_t f0 = half2_bits(v.re * ph, -v.im * ph), f1 = half2_bits(v.im * ph, v.re * ph);
+        *reinterpret_cast<uint4 *>(sVar + bt * 4) = make_uint4(f0, f0 ^ 0x80008000u, f1, f1 ^ 0x80008000u);
+      }
+      builders_sync();
+      uint8_t *wslot = smem + k * S::SLOT;
 #pragma unroll
-    for (int m = 0; m < MT_SEG_SLOTS; m++)
-      if (segon[m])
-        *reinterpret_cast<uint4 *>(smem + bslot + segoff[m]) =
-            make_uint4(sVar[segw[m][0]], sVar[segw[m][1]], sVar[segw[m][2]], sVar[segw[m][3]]);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // B visible to the tensor core
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    ok = __syncthreads_and(ok);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!ok) break;
-    // (4) the site's 16 MMAs, once its A tiles have landed
-    if (tid == 0) {
-      const bool landed = mbar_wait(smem_u32(&bars[slot]), (i >> 1) & 1);
-      if (landed) {
-        a_done[slot]++;
+      for (int m = 0; m < MT_SEG_SLOTS; m++)
+        if (segon[m])
+          *reinterpret_cast<uint4 *>(wslot + segoff[m]) =
+              make_uint4(sVar[segw[m][0]], sVar[segw[m][1]], sVar[segw[m][2]], sVar[segw[m][3]]);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // B visible to the tensor core
+      __syncwarp();
+      if (lane == 0) mbar_arrive(bar_bready(k));  // one arrival per builder warp
+    }
+  } else if (warp == MT_MMA_WARP) {
+    // ---------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_f16<128, 32>(false);
+      int last_bar = -1, last_par = 0;
+      for (int i = 0; i < nloc; i++) {
+        const int k = i % NS, u = i / NS, d = i % MT_ND, ud = i / MT_ND;
+        if (!mt_wait(bar_bready(k), u & 1, abort_flag) || !mt_wait(bar_full(k), u & 1, abort_flag) ||
+            (ud >= 1 && !mt_wait(bar_dempty(d), (ud - 1) & 1, abort_flag))) {
+          fail();
+          break;
+        }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t base = s0 + k * S::SLOT;
+        // the 8 tiles are one run of 24 K-chunks (chunk c of hop h at (3 h + c) LBO): K = 192 in 12 steps
 #pragma unroll
-        for (int h = 0; h < MT_HOPS; h++)
-#pragma unroll
-          for (int ks = 0; ks < 2; ks++) {
-            const uint64_t ad = umma_desc(a_addr(slot, h) + ks * 2 * (16 * RP), 16 * RP, 128);
-            const uint64_t bd = umma_desc(b_addr(slot, h) + ks * 256, 128, 512);
-            umma_f16(tmem + slot * 32, ad, bd, idesc, (h > 0 || ks > 0) ? 1u : 0u);
-          }
-        umma_commit(smem_u32(&bars[2 + slot]));
-        m_iss[slot]++;
+        for (int ks = 0; ks < MT_K / 16; ks++) {
+          const uint64_t ad = umma_desc(base + ks * 2 * (16 * RP), 16 * RP, 128);
+          const uint64_t bd = umma_desc(base + S::A_BYTES + ks * 256, 128, MT_K / 8 * 128);
+          umma_f16(tmem + d * 32, ad, bd, idesc, ks > 0 ? 1u : 0u);
+        }
+        umma_commit(bar_mdone(k));
+        umma_commit(bar_dfull(d));
+        last_bar = k;
+        last_par = u & 1;
       }
-      ok = landed;
+      // every MMA issued is complete before the tensor memory is freed
+      if (last_bar >= 0 && !mbar_wait(bar_mdone(last_bar), last_par)) atomicExch(a.err, 1);
     }
-    // (5) epilogue of the previous site
-    if (i >= 1 && warp * 32 < RP) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      float d0[16], d1[16];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (slot ^ 1) * 32;
-      tmem_ld16(taddr, d0);
-      tmem_ld16(taddr + 16, d1);
-      const int row = warp * 32 + lane;
-      uint4 *o = reinterpret_cast<uint4 *>(a.out + (size_t)s_prev * (24 * RP) + row * 8);
-      o[0] = make_uint4(half2_bits(d0[0], d0[1]), half2_bits(d0[2], d0[3]), half2_bits(d0[4], d0[5]),
-                        half2_bits(d0[6], d0[7]));
-      o[RP] = make_uint4(half2_bits(d0[8], d0[9]), half2_bits(d0[10], d0[11]), half2_bits(d0[12], d0[13]),
-                         half2_bits(d0[14], d0[15]));
-      o[2 * RP] = make_uint4(half2_bits(d1[0], d1[1]), half2_bits(d1[2], d1[3]), half2_bits(d1[4], d1[5]),
-                             half2_bits(d1[6], d1[7]));
-    }
-    s_prev = s_cur;
-    // the accumulators just read are overwritten by the MMAs of site i + 1 only after this barrier
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    ok = __syncthreads_and(ok);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  }
-  // the last site's epilogue
-  if (ok && nloc > 0) {
-    const int slot = (nloc - 1) & 1;
-    ok = mbar_wait(smem_u32(&bars[2 + slot]), ((nloc - 1) >> 1) & 1);
-    if (ok) m_done[slot]++;
-    // tcgen05.ld is warp-collective: a warp reads only if all its threads saw the MMAs complete
-    if (__all_sync(0xffffffffu, ok) && warp * 32 < RP) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      float d0[16], d1[16];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + slot * 32;
-      tmem_ld16(taddr, d0);
-      tmem_ld16(taddr + 16, d1);
-      const int row = warp * 32 + lane;
-      uint4 *o = reinterpret_cast<uint4 *>(a.out + (size_t)s_prev * (24 * RP) + row * 8);
-      o[0] = make_uint4(half2_bits(d0[0], d0[1]), half2_bits(d0[2], d0[3]), half2_bits(d0[4], d0[5]),
-                        half2_bits(d0[6], d0[7]));
-      o[RP] = make_uint4(half2_bits(d0[8], d0[9]), half2_bits(d0[10], d0[11]), half2_bits(d0[12], d0[13]),
-                         half2_bits(d0[14], d0[15]));
-      o[2 * RP] = make_uint4(half2_bits(d1[0], d1[1]), half2_bits(d1[2], d1[3]), half2_bits(d1[4], d1[5]),
-                             half2_bits(d1[6], d1[7]));
-    }
-  }
-  if (!ok) atomicExch(a.err, 1);
-  // drain: every MMA batch thread 0 issued must be done before the tensor
-  // memory is freed, and every bulk copy before the shared memory goes away
-  // (bounded waits, completions in order)
-  if (tid == 0) {
-    for (int k = 0; k < 2; k++) {
-      while (a_done[k] < a_iss[k]) {
-        if (!mbar_wait(smem_u32(&bars[k]), a_done[k] & 1)) atomicExch(a.err, 1);
-        a_done[k]++;
-      }
-      while (m_done[k] < m_iss[k]) {
-        if (!mbar_wait(smem_u32(&bars[2 + k]), m_done[k] & 1)) atomicExch(a.err, 1);
-        m_done[k]++;
+  } else {
+    // ---------------------------------------------------------- epilogue
+    const int qd = warp & 3;  // tensor-memory lane quarter of this warp
+    if (qd * 32 < RP) {
+      for (int i = 0; i < nloc; i++) {
+        const int d = i % MT_ND, ud = i / MT_ND;
+        const bool ok = __all_sync(0xffffffffu, mt_wait(bar_dfull(d), ud & 1, abort_flag));
+        if (!ok) {
+          if (lane == 0) fail();
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        float d0[16], d1[16];
+        const uint32_t taddr = tmem + ((uint32_t)(qd * 32) << 16) + d * 32;
+        tmem_ld16(taddr, d0);
+        tmem_ld16(taddr + 16, d1);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar_dempty(d));  // the accumulators are read: the slot is free
+        const int s = mt_site(a, q_of(i)).s;
+        const int row = qd * 32 + lane;
+        uint4 *o = reinterpret_cast<uint4 *>(a.out + (size_t)s * (24 * RP) + row * 8);
+        o[0] = make_uint4(half2_bits(d0[0], d0[1]), half2_bits(d0[2], d0[3]), half2_bits(d0[4], d0[5]),
+                          half2_bits(d0[6], d0[7]));
+        o[RP] = make_uint4(half2_bits(d0[8], d0[9]), half2_bits(d0[10], d0[11]), half2_bits(d0[12], d0[13]),
+                           half2_bits(d0[14], d0[15]));
+        o[2 * RP] = make_uint4(half2_bits(d1[0], d1[1]), half2_bits(d1[2], d1[3]), half2_bits(d1[4], d1[5]),
+                               half2_bits(d1[6], d1[7]));
       }
     }
   }
@@ -379,7 +460,7 @@ __global__ void __launch_bounds__(MT_THREADS) k_mrhs_tc(MtArgs a) {
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64u) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u * MT_ND) : "memory");
   }
 }
 
@@ -448,7 +529,7 @@ void launch_mt(const MtArgs &a, int sms, cudaStream_t s) {
   auto k = k_mrhs_tc<RP>;
   QCU_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
   QCU_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
-  const int grid = std::min(a.g.Vh, sms * S::CTAS_PER_SM);
+  const int grid = std::min(a.g.Vh, sms);  // one CTA per SM (its shared memory)
   k<<<grid, MT_THREADS, S::SMEM, s>>>(a);
   QCU_CHECK_LAUNCH();
 }
@@ -469,6 +550,14 @@ void launch_mrhs_tc(const Geom &g, const void *gauge16, double t_bc, const void 
   a.out = static_cast<__half *>(out);
   a.par = par;
   a.zb = g.Lz % 8 == 0 ? 8 : (g.Lz % 4 == 0 ? 4 : (g.Lz % 2 == 0 ? 2 : 1));
+  auto magic = [&](int d) -> unsigned {  // exact for every q < Vh while (Vh + 64) d < 2^32 (geom_div)
+    if (d < 2 || (uint64_t)(g.Vh + 64) * (uint64_t)d >= (1ULL << 32)) return 0u;
+    return (unsigned)(((1ULL << 32) + (uint64_t)d - 1) / (uint64_t)d);
+  };
+  a.m_plane = magic(g.Ly * g.Lxh);
+  a.m_zb = magic(a.zb);
+  a.m_lt = magic(g.Lt);
+  a.m_lxh = magic(g.Lxh);
   a.err = err;
   if (mrhs_rows(nrhs) == 64) launch_mt<64>(a, sms, s);
   else launch_mt<128>(a, sms, s);
