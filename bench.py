@@ -22,7 +22,8 @@ end-to-end time through the C ABI from host buffers, the clover target
 every storage precision with errors against the CPU oracle's FP64 solve, the
 learned preconditioner, the batched multi-RHS solve, the two-level
 multigrid (set-up, its own solve, and the chosen solver with its coarse-grid
-correction), and a CPU baseline (the FP64 CPU oracle on all host cores,
+correction), the multi-right-hand-side hopping term on the tcgen05 tensor
+cores against the batched FMA kernel, and a CPU baseline (the FP64 CPU oracle on all host cores,
 bounded sample).
 
 `--impl reference` times one complete FP64 solve of the CPU restatement of
@@ -470,6 +471,44 @@ def multigrid_block(args, q, G, b, x, stream, chosen_kw):
         mg.close()
 
 
+def multi_rhs_tc_block(q, G, latt):
+    """The multi-right-hand-side hopping term on the tcgen05 tensor cores
+    (FP16 operands, FP32 accumulation) on the benchmark gauge field, 64 and 128
+    right-hand sides, against the batched FMA kernel (autotuned shape, FP32
+    spinors with 16-bit links and 16-bit spinors) on the same 64 right-hand
+    sides of a 16^3 x 32 system, where the FMA batch fits in memory; device
+    time per application with CUDA events, and per right-hand-side site."""
+    import torch
+
+    vh = latt[0] * latt[1] * latt[2] * latt[3] // 2
+    out = {"operator": "D_{0<-1} on nrhs half spinors", "lattice": "x".join(map(str, latt)), "rows": []}
+    for n in (64, 128):
+        ms = G.dslash_multi_tc_time(n, 0, iters=10)
+        out["rows"].append({"nrhs": n, "tc_ms": round(ms, 4), "tc_ps_per_rhs_site": round(ms * 1e9 / (vh * n), 2)})
+    small = [16, 16, 16, 32]
+    Ls = q.Layout(tuple(small))
+    us = torch.empty(Ls.gauge, dtype=torch.complex128, device="cuda")
+    q.gauge_random(us, small, 1, 0.25, 5)
+    with q.Gauge(us, small, t_boundary=-1.0) as Gs:
+        cmp = {"lattice": "16x16x16x32", "nrhs": 64}
+        ms = Gs.dslash_multi_tc_time(64, 0, iters=10)
+        cmp["tc_ps_per_rhs_site"] = round(ms * 1e9 / (Ls.vh * 64), 2)
+        ms = Gs.dslash_multi_tc_time(128, 0, iters=10)
+        cmp["tc_128rhs_ps_per_rhs_site"] = round(ms * 1e9 / (Ls.vh * 128), 2)
+        bb = torch.empty((64,) + tuple(Ls.full), dtype=torch.complex128, device="cuda")
+        q.fermion_random(bb, bb.numel(), 0, 11)
+        xx = torch.zeros_like(bb)
+        for name, prec, gp in (("fma_fp32_links16", 32, 16), ("fma_16bit", 16, 0)):
+            ms, tune = q.batch_dslash_time([(Gs, xx, bb, 0.12, False)], precision=prec, gauge_precision=gp, iters=10)
+            cmp[name + "_ps_per_rhs_site"] = round(ms * 1e9 / (Ls.vh * 64), 2)
+            cmp[name + "_tune"] = tune
+        del bb, xx
+    del us
+    torch.cuda.empty_cache()
+    out["vs_batched_fma"] = cmp
+    return out
+
+
 def batch_config(args, q, stream, chosen_kw):
     """Batched multi-RHS workload: the 12 point sources of a propagator on
     32^3 x 64 clover (csw = 1) together with 4 Gaussian right-hand sides on
@@ -829,6 +868,7 @@ def run_ours(args, world, rank, local, pg):
         extra["learned"] = learned_block(q, lib_stream, chosen_kw, gauge, b, latt)
         extra["batch"] = batch_config(args, q, lib_stream, chosen_kw)
         extra["multigrid"] = multigrid_block(args, q, G, b, x, lib_stream, chosen_kw)
+        extra["multi_rhs_tc"] = multi_rhs_tc_block(q, G, latt)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
