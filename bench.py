@@ -62,7 +62,7 @@ DSLASH_BYTES = {"64": 192 + 8 * 96 + 192, "32": 96 + 8 * 48 + 96, "16": 52 + 8 *
 DSLASH_FLOPS = 1320
 # DRAM bytes (read + write) per launch of each dslash storage at 32^3 x 64 from
 # one ncu capture each (profiles/k_dslash_*_32x32x32x64.txt)
-DSLASH_TRAFFIC = {"16": {"bytes": 296_890_000, "profile": "profiles/k_dslash_soa16_gsoa16_32x32x32x64.txt"},
+DSLASH_TRAFFIC = {"16": {"bytes": 298_198_016, "profile": "profiles/k_dslash_soa16_gsoa16_32x32x32x64.txt"},
                   "32/16": {"bytes": 387_940_000, "profile": "profiles/k_dslash_soa32_gsoa16_32x32x32x64.txt"},
                   "64": {"bytes": 1_208_100_000, "profile": "profiles/k_dslash_soa64_32x32x32x64.txt"}}
 
