@@ -79,7 +79,7 @@ def parse():
     ap.add_argument("--gauge-precision", type=int, default=None, choices=[0, 16],
                     help="16: FP32 spinors with 16-bit links (default 16 with --precision 32, else 0)")
     ap.add_argument("--inner-iters", type=int, default=96)
-    ap.add_argument("--inner-tol", type=float, default=0.05)
+    ap.add_argument("--inner-tol", type=float, default=0.03)
     ap.add_argument("--gcr-k", type=int, default=4)
     ap.add_argument("--kappa", type=float, default=KAPPA)
     ap.add_argument("--latt", type=int, nargs=4, default=LATT)
@@ -660,7 +660,7 @@ def clover_c3_block(q, stream):
     t_oracle = time.perf_counter() - t0
     res_o = float(np.linalg.norm(b - O.mfull(xo, U, latt, kappa, T_BC, True, A[0], A[1])) / np.linalg.norm(b))
     del A, Ainv
-    gcr = dict(solver="gcr", inner_iters=96, inner_tol=0.05, gcr_k=4)
+    gcr = dict(solver="gcr", inner_iters=96, inner_tol=0.03, gcr_k=4)
     methods = [("plain FP64 BiCGSTAB", dict(precision=64, delta=0.0)),
                ("BiCGSTAB FP32 storage, FP64 reliable updates", dict(precision=32, delta=0.1)),
                ("BiCGSTAB 16-bit storage, FP64 reliable updates", dict(precision=16, delta=0.1)),

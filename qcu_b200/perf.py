@@ -75,11 +75,12 @@ def main(argv=None):
     ap.add_argument("--csw", type=float, default=0.0)
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--repeat", type=int, default=1, help="solve: solves to time (median of all but the first)")
+    ap.add_argument("--src-seed", type=int, default=7, help="solve: seed of the Gaussian source")
     ap.add_argument("--kappa", type=float, default=0.1303)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--solver", default="gcr", choices=["gcr", "bicgstab"])
     ap.add_argument("--inner-iters", type=int, default=96)
-    ap.add_argument("--inner-tol", type=float, default=0.05)
+    ap.add_argument("--inner-tol", type=float, default=0.03)
     ap.add_argument("--gcr-k", type=int, default=4)
     ap.add_argument("--single", action="store_true", help="batch: also time the 24 systems one at a time")
     ap.add_argument("--only-point", action="store_true", help="batch: only the 12 point sources on --latt")
@@ -175,7 +176,7 @@ def main(argv=None):
         return
     G, u, L = _gauge(a.latt, a.eps, a.seed, a.t_bc, a.csw, a.kappa)
     b = torch.empty(L.full, dtype=torch.complex128, device="cuda")
-    q.fermion_random(b, b.numel(), 0, 7)
+    q.fermion_random(b, b.numel(), 0, a.src_seed)
     x = torch.empty_like(b)
     times = []
     for _ in range(max(1, a.repeat)):
