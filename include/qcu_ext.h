@@ -142,7 +142,9 @@ int qcuBatchDslashTime(const qcuBatchSystem *systems, int n_systems, int precisi
  * hop one tensor-core product serves every right-hand side: spinors are
  * rounded to FP16 once, B = real form of (1 -+ gamma_mu) x U in FP16 (from the
  * 16-bit links), FP32 accumulation; the result is rounded to FP16 (about
- * 1e-3 relative, against 1e-6 for the FP32 hop). */
+ * 1e-3 relative, against 1e-6 for the FP32 hop).  Two FP16 work fields of
+ * Vh x 48 x (64 or 128) bytes are kept per device for reuse (the library's
+ * memory pool). */
 int qcuDslashMultiTC(qcuGauge h, void *out, const void *in, int nrhs, int parity);
 /* its kernel alone, on resident seeded multi-rhs fields: *ms = mean device
  * time per application over `iters` launches (CUDA events) */
