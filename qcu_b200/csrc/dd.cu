@@ -14,11 +14,13 @@
 //      by its own link, U_mu(x)^dag (1 + gamma_mu) psi (the link lives on the
 //      sending rank).  Six complex numbers per face site cross the link
 //      instead of twelve.
-//   2. the faces are exchanged: NCCL point-to-point on the library stream
+//   2. the faces are exchanged on a stream of their own: NCCL point-to-point
 //      (grouped send/recv to the two neighbours of every partitioned
 //      direction), or device-to-device copies when all ranks of a grid are
 //      emulated in one process on one GPU (qcuDslashDDEmulate, the test of
-//      the kernels and the exchange schedule without a second GPU);
+//      the kernels and the exchange schedule without a second GPU); the
+//      interior sites, whose hops read no face, are computed meanwhile on
+//      the library stream, the boundary sites once the faces have landed;
 //   3. k_dd_dslash: one thread per output site, the eight hops in the order
 //      of the single-GPU kernel; a hop that crosses a partitioned boundary
 //      reads the received face (forward: multiply by the local link;
@@ -261,14 +263,29 @@ __device__ __forceinline__ void dd_hop(Cpx<double> acc[12], const DDDev &d, cons
   dd_reconstruct<MU, FWD>(acc, uh);
 }
 
+// a site on the face of a partitioned direction: one of its hops reads a received face
+__device__ __forceinline__ bool dd_on_face(const DDDev &d, const Coord &c) {
+  bool on = false;
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) {
+    const int pos = mu == 0 ? c.x : (mu == 1 ? c.y : (mu == 2 ? c.z : c.t));
+    const int L = mu == 0 ? 2 * d.g.Lxh : (mu == 1 ? d.g.Ly : (mu == 2 ? d.g.Lz : d.g.Lt));
+    on |= (d.part >> mu & 1) && (pos == 0 || pos == L - 1);
+  }
+  return on;
+}
+
+// mode 0: every output site; 1: the interior (no hop reads a received face),
+// which runs while the faces are in flight; 2: the boundary, after they landed
 __global__ void __launch_bounds__(DSLASH_BLOCK, 3)
-    k_dd_dslash(DDDev d, const double2 *__restrict__ in, const void *gauge, double2 *out, int par) {
+    k_dd_dslash(DDDev d, const double2 *__restrict__ in, const void *gauge, double2 *out, int par, int mode) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= d.g.Vh) return;
   const Geom &g = d.g;
   const SpinorView<AOS64> inv{const_cast<double2 *>(in), nullptr, g.Vh};
   const GaugeView<GAOS64> U{gauge, g.Vh};
   const Coord c = dd_coord(g, s, par);
+  if (mode != 0 && dd_on_face(d, c) != (mode == 2)) return;
   const int xh = c.x >> 1, xodd = c.x & 1;
   Cpx<double> acc[12];
 #pragma unroll
@@ -425,6 +442,19 @@ struct DDComm {
 };
 DDComm &comm_of(const Context &ctx) { return per_device<DDComm>(ctx); }
 
+// the stream the faces travel on, beside the library stream, and the two
+// events that order it: faces packed -> exchange; exchange done -> boundary
+struct DDStreams {
+  cudaStream_t comm = nullptr;
+  cudaEvent_t packed = nullptr, landed = nullptr;
+  void ensure() {
+    if (comm) return;
+    QCU_CUDA(cudaStreamCreateWithFlags(&comm, cudaStreamNonBlocking));
+    QCU_CUDA(cudaEventCreateWithFlags(&packed, cudaEventDisableTiming));
+    QCU_CUDA(cudaEventCreateWithFlags(&landed, cudaEventDisableTiming));
+  }
+};
+
 // The distributed operators on this process's ranks: every rank of the grid
 // (emulated, faces exchanged by device copies) or this process's one rank
 // (faces exchanged with NCCL).  The caller holds the context lock.
@@ -455,13 +485,27 @@ class DDRun {
   const DDPlan &plan(int r) const { return plans_[r]; }
   const DDDev &dev(int r) const { return dev_[r]; }
 
-  // out[r] = D_{par <- 1-par} in[r] on every domain (PyQuda-layout halves)
+  // out[r] = D_{par <- 1-par} in[r] on every domain (PyQuda-layout halves).
+  // The faces are packed on the library stream and exchanged on a stream of
+  // their own while the interior sites are computed; the boundary sites
+  // follow once the faces have landed.
   void dslash(int par, const std::vector<const void *> &gauge, const std::vector<const void *> &in,
               const std::vector<void *> &out) {
     const cudaStream_t st = ctx_.stream;
+    if (dev_[0].part == 0) {  // nothing partitioned: one pass, no exchange
+      for (int r = 0; r < domains(); r++) launch_dd_dslash(dev_[r], in[r], gauge[r], out[r], par, 0, st);
+      return;
+    }
+    DDStreams &ss = per_device<DDStreams>(ctx_);
+    ss.ensure();
     for (int r = 0; r < domains(); r++) launch_pack(dev_[r], in[r], gauge[r], 1 - par, st);
-    exchange();
-    for (int r = 0; r < domains(); r++) launch_dd_dslash(dev_[r], in[r], gauge[r], out[r], par, st);
+    QCU_CUDA(cudaEventRecord(ss.packed, st));
+    QCU_CUDA(cudaStreamWaitEvent(ss.comm, ss.packed, 0));
+    exchange(ss.comm);
+    QCU_CUDA(cudaEventRecord(ss.landed, ss.comm));
+    for (int r = 0; r < domains(); r++) launch_dd_dslash(dev_[r], in[r], gauge[r], out[r], par, 1, st);
+    QCU_CUDA(cudaStreamWaitEvent(st, ss.landed, 0));
+    for (int r = 0; r < domains(); r++) launch_dd_dslash(dev_[r], in[r], gauge[r], out[r], par, 2, st);
   }
 
   // v[0..n) summed over all ranks of the grid (over the domains of this
@@ -482,8 +526,7 @@ class DDRun {
   }
 
  private:
-  void exchange() {
-    const cudaStream_t st = ctx_.stream;
+  void exchange(cudaStream_t st) {
     if (!emulate_) {
       NcclApi &n = nccl();
       const std::vector<DDOp> ops = dd_schedule(plans_[0]);
@@ -534,10 +577,10 @@ class DDRun {
         d, static_cast<const double2 *>(in), gauge, par);
     QCU_CHECK_LAUNCH();
   }
-  static void launch_dd_dslash(const DDDev &d, const void *in, const void *gauge, void *out, int par,
+  static void launch_dd_dslash(const DDDev &d, const void *in, const void *gauge, void *out, int par, int mode,
                                cudaStream_t s) {
     k_dd_dslash<<<(d.g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK, DSLASH_BLOCK, 0, s>>>(
-        d, static_cast<const double2 *>(in), gauge, static_cast<double2 *>(out), par);
+        d, static_cast<const double2 *>(in), gauge, static_cast<double2 *>(out), par, mode);
     QCU_CHECK_LAUNCH();
   }
 
