@@ -22,9 +22,9 @@
 // of 8 rows x 16 B, LBO = 16 RP B between K-chunks, SBO = 128 B between
 // 8-row groups), so one bulk copy brings a neighbour's whole A tile.
 //
-// One CTA per SM, persistent over sites, with warp roles joined only by
-// mbarriers, so that loads, B builds, MMAs and read-back of different sites
-// overlap (3 or 4 site slots, four accumulator slots):
+// Persistent CTAs (two per SM for 64 rows, one for 128: shared memory), with
+// warp roles joined only by mbarriers, so that loads, B builds, MMAs and
+// read-back of different sites overlap (3 site slots, four accumulator slots):
 //   * warps 0-3 load, running ahead of the others: per site the 8
 //     neighbours' A tiles as 16-byte cp.async pieces (a warp moves 512
 //     contiguous bytes per step; one bulk-copy engine per SM issued them
@@ -92,7 +92,8 @@ struct MtShape {
   static constexpr int OFF_L8 = OFF_L16 + MT_HOPS * 16;
   static constexpr int OFF_PH = OFF_L8 + MT_HOPS * 8;
   static constexpr int SLOT = (OFF_PH + MT_HOPS * 4 + 1023) / 1024 * 1024;
-  static constexpr int NS = RP == 64 ? 4 : 3;  // site slots (shared memory: 4 x 37 KB or 3 x 61 KB)
+  static constexpr int NS = 3;  // site slots (shared memory: 3 x 37 KB or 3 x 61 KB)
+  static constexpr int CTAS_PER_SM = RP == 64 ? 2 : 1;  // 64 rows: two pipelines per SM
   static constexpr int OFF_VAR = NS * SLOT;    // builders' scratch: the pairs of the 8 links' elements
   static constexpr int OFF_BAR = OFF_VAR + (MT_NVAR + 4) * 4;
   // mbarriers: full[NS] (A tiles + link words landed), bready[NS] (B built),
@@ -208,7 +209,7 @@ __device__ __forceinline__ int mt_pair_word(int h, int n, int k2) {
 }
 
 template <int RP>
-__global__ void __launch_bounds__(MT_THREADS, 1) k_mrhs_tc(MtArgs a) {
+__global__ void __launch_bounds__(MT_THREADS, MtShape<RP>::CTAS_PER_SM) k_mrhs_tc(MtArgs a) {
   using S = MtShape<RP>;
   constexpr int NS = S::NS;
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -529,7 +530,7 @@ void launch_mt(const MtArgs &a, int sms, cudaStream_t s) {
   auto k = k_mrhs_tc<RP>;
   QCU_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, S::SMEM));
   QCU_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
-  const int grid = std::min(a.g.Vh, sms);  // one CTA per SM (its shared memory)
+  const int grid = std::min(a.g.Vh, sms * S::CTAS_PER_SM);  // as many CTAs as shared memory holds
   k<<<grid, MT_THREADS, S::SMEM, s>>>(a);
   QCU_CHECK_LAUNCH();
 }
