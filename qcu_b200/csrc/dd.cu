@@ -20,7 +20,8 @@
 //      emulated in one process on one GPU (qcuDslashDDEmulate, the test of
 //      the kernels and the exchange schedule without a second GPU); the
 //      interior sites, whose hops read no face, are computed meanwhile on
-//      the library stream, the boundary sites once the faces have landed;
+//      the library stream, the boundary sites (a list built once per
+//      lattice, partition and parity) once the faces have landed;
 //   3. k_dd_dslash: one thread per output site, the eight hops in the order
 //      of the single-GPU kernel; a hop that crosses a partitioned boundary
 //      reads the received face (forward: multiply by the local link;
@@ -275,17 +276,32 @@ __device__ __forceinline__ bool dd_on_face(const DDDev &d, const Coord &c) {
   return on;
 }
 
-// mode 0: every output site; 1: the interior (no hop reads a received face),
-// which runs while the faces are in flight; 2: the boundary, after they landed
-__global__ void __launch_bounds__(DSLASH_BLOCK, 3)
-    k_dd_dslash(DDDev d, const double2 *__restrict__ in, const void *gauge, double2 *out, int par, int mode) {
+// the output sites of parity par that read a received face (any order: each
+// site is computed on its own)
+__global__ void k_dd_boundary_list(DDDev d, int par, int *list, int *count) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= d.g.Vh) return;
+  if (dd_on_face(d, dd_coord(d.g, s, par))) list[atomicAdd(count, 1)] = s;
+}
+
+// mode 0: every output site; 1: the interior (no hop reads a received face),
+// which runs while the faces are in flight; 2: the nlist boundary sites of
+// list, after the faces landed
+__global__ void __launch_bounds__(DSLASH_BLOCK, 3)
+    k_dd_dslash(DDDev d, const double2 *__restrict__ in, const void *gauge, double2 *out, int par, int mode,
+                const int *list, int nlist) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (mode == 2) {
+    if (s >= nlist) return;
+    s = list[s];
+  } else if (s >= d.g.Vh) {
+    return;
+  }
   const Geom &g = d.g;
   const SpinorView<AOS64> inv{const_cast<double2 *>(in), nullptr, g.Vh};
   const GaugeView<GAOS64> U{gauge, g.Vh};
   const Coord c = dd_coord(g, s, par);
-  if (mode != 0 && dd_on_face(d, c) != (mode == 2)) return;
+  if (mode == 1 && dd_on_face(d, c)) return;
   const int xh = c.x >> 1, xodd = c.x & 1;
   Cpx<double> acc[12];
 #pragma unroll
@@ -387,8 +403,16 @@ struct DDBufs {
     return d;
   }
 };
+// the boundary sites of one output parity (the same on every rank: equal
+// local lattices and partitioned directions), built on first use
+struct DDBoundary {
+  DevBuf list, count;
+  int n = -1;
+  int key[5] = {0, 0, 0, 0, -1};  // Lxh, Ly, Lz, Lt, partitioned directions
+};
 struct DDSpace {
   std::vector<std::unique_ptr<DDBufs>> ranks;
+  DDBoundary bnd[2];
   DDBufs &at(int r) {
     while ((int)ranks.size() <= r) ranks.push_back(std::make_unique<DDBufs>());
     return *ranks[r];
@@ -498,6 +522,7 @@ class DDRun {
     }
     DDStreams &ss = per_device<DDStreams>(ctx_);
     ss.ensure();
+    const DDBoundary &bl = boundary(par);
     for (int r = 0; r < domains(); r++) launch_pack(dev_[r], in[r], gauge[r], 1 - par, st);
     QCU_CUDA(cudaEventRecord(ss.packed, st));
     QCU_CUDA(cudaStreamWaitEvent(ss.comm, ss.packed, 0));
@@ -505,7 +530,8 @@ class DDRun {
     QCU_CUDA(cudaEventRecord(ss.landed, ss.comm));
     for (int r = 0; r < domains(); r++) launch_dd_dslash(dev_[r], in[r], gauge[r], out[r], par, 1, st);
     QCU_CUDA(cudaStreamWaitEvent(st, ss.landed, 0));
-    for (int r = 0; r < domains(); r++) launch_dd_dslash(dev_[r], in[r], gauge[r], out[r], par, 2, st);
+    for (int r = 0; r < domains(); r++)
+      launch_dd_dslash(dev_[r], in[r], gauge[r], out[r], par, 2, st, bl.list.as<int>(), bl.n);
   }
 
   // v[0..n) summed over all ranks of the grid (over the domains of this
@@ -578,10 +604,30 @@ class DDRun {
     QCU_CHECK_LAUNCH();
   }
   static void launch_dd_dslash(const DDDev &d, const void *in, const void *gauge, void *out, int par, int mode,
-                               cudaStream_t s) {
-    k_dd_dslash<<<(d.g.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK, DSLASH_BLOCK, 0, s>>>(
-        d, static_cast<const double2 *>(in), gauge, static_cast<double2 *>(out), par, mode);
+                               cudaStream_t s, const int *list = nullptr, int nlist = 0) {
+    const int n = mode == 2 ? nlist : d.g.Vh;
+    if (n <= 0) return;
+    k_dd_dslash<<<(n + DSLASH_BLOCK - 1) / DSLASH_BLOCK, DSLASH_BLOCK, 0, s>>>(
+        d, static_cast<const double2 *>(in), gauge, static_cast<double2 *>(out), par, mode, list, nlist);
     QCU_CHECK_LAUNCH();
+  }
+  // the boundary sites of output parity par, built once per lattice and partition
+  const DDBoundary &boundary(int par) {
+    DDBoundary &b = per_device<DDSpace>(ctx_).bnd[par];
+    const int key[5] = {g_.Lxh, g_.Ly, g_.Lz, g_.Lt, dev_[0].part};
+    if (b.n >= 0 && std::equal(key, key + 5, b.key)) return b;
+    b.list.ensure((size_t)g_.Vh * sizeof(int));
+    b.count.ensure(sizeof(int));
+    QCU_CUDA(cudaMemsetAsync(b.count.p, 0, sizeof(int), ctx_.stream));
+    k_dd_boundary_list<<<(g_.Vh + DSLASH_BLOCK - 1) / DSLASH_BLOCK, DSLASH_BLOCK, 0, ctx_.stream>>>(
+        dev_[0], par, b.list.as<int>(), b.count.as<int>());
+    QCU_CHECK_LAUNCH();
+    int n = 0;
+    QCU_CUDA(cudaMemcpyAsync(&n, b.count.p, sizeof(int), cudaMemcpyDeviceToHost, ctx_.stream));
+    QCU_CUDA(cudaStreamSynchronize(ctx_.stream));
+    b.n = n;
+    std::copy(key, key + 5, b.key);
+    return b;
   }
 
   Context &ctx_;
