@@ -148,7 +148,7 @@ std::vector<SolveInfo> solve_batch(const std::vector<BatchSystem> &sys, const So
     const GaugeHandle &G = *s.G;
     RhsBufs &B = *c.rhs[r];
     RhsDesc &d = desc[r];
-    memset(&d, 0, sizeof(d));
+    d = RhsDesc{};
     d.g = G.g;
     d.kappa = s.kappa;
     d.k2 = s.kappa * s.kappa;
