@@ -29,18 +29,25 @@ namespace qcu {
 #define QCU_DSLASH32_BLOCKS 7  // FP32 / 16-bit spinors without a reduction
 #endif
 #ifndef QCU_DSLASH16_RED_BLOCKS
-#define QCU_DSLASH16_RED_BLOCKS 6  // 16-bit spinors with a reduction
+#define QCU_DSLASH16_RED_BLOCKS 7  // 16-bit spinors with a reduction
+#endif
+#ifndef QCU_DSLASH16_CLOV_RED_BLOCKS
+#define QCU_DSLASH16_CLOV_RED_BLOCKS 6  // the same with the clover term
 #endif
 // 16-bit spinors reduce in two kernels: every block of the dslash writes its
 // partial, and a one-block kernel sums them.  The strided one-wave form
-// (every other kind) takes ~165 registers there and 3 resident blocks; the
-// split form fits 80 registers and 6 blocks, which measured faster for the
-// 16-bit kernels and slower for the FP32 ones.
+// (every other kind) takes ~165 registers there and 3 resident blocks.  The
+// split form measured faster for the 16-bit kernels and slower for the FP32
+// ones.  It fits 72 registers and 7 blocks (4-8 bytes spilled), which made a
+// solve 0.5 % faster than 80 registers and 6 blocks; with the clover term 7
+// blocks would spill 52-68 bytes, so those keep 80 registers and 6 blocks.
 #define DSLASH_SPLIT_RED(K) ((K) == SOA16)
 #define DSLASH_RED_BLOCKS(K) ((K) == SOA16 ? QCU_DSLASH16_RED_BLOCKS : 3)
-#define DSLASH_MIN_BLOCKS(K, RED)                     \
-  (((K) == AOS64 || (K) == AOS64W || (K) == SOA64) ? 3 \
-                                                   : ((RED) == RED_NONE ? QCU_DSLASH32_BLOCKS : DSLASH_RED_BLOCKS(K)))
+#define DSLASH_MIN_BLOCKS(K, RED, CLOV)                                                   \
+  (((K) == AOS64 || (K) == AOS64W || (K) == SOA64) ? 3                                   \
+   : (RED) == RED_NONE                            ? QCU_DSLASH32_BLOCKS                  \
+   : ((K) == SOA16 && (CLOV))                     ? QCU_DSLASH16_CLOV_RED_BLOCKS         \
+                                                  : DSLASH_RED_BLOCKS(K))
 
 // FP32 and 16-bit spinors: the hop and the epilogue on spin-paired registers
 // in FP32 arithmetic (hop32.cuh)
@@ -139,7 +146,7 @@ __device__ __forceinline__ void dslash_site_scalar(const Geom &g, const DslashAr
 }
 
 template <int K, int G, int C, bool CLOV, int NX, int RED>
-__global__ void __launch_bounds__(DSLASH_BLOCK, DSLASH_MIN_BLOCKS(K, RED)) k_dslash(Geom g, DslashArgs a, RedCtx rc) {
+__global__ void __launch_bounds__(DSLASH_BLOCK, DSLASH_MIN_BLOCKS(K, RED, CLOV)) k_dslash(Geom g, DslashArgs a, RedCtx rc) {
   if (!gate_open(rc.st, a.gate)) return;
   constexpr int NV = RED == RED_NONE ? 1 : (RED == RED_TS_TT ? 3 : (RED == RED_DOT_RT ? 2 : 1));
   double red[NV];
